@@ -1,0 +1,153 @@
+"""CPU oracle checks: pinned against the reference's own tables and source,
+against mpmath, SciPy quadrature and dense linear algebra."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_gauss_legendre_matches_reference_table(oracle_mod):
+    g = json.load(open(os.path.join(GOLDEN, "gauss_legendre_10.json")))
+    x, w = oracle_mod.gauss_legendre(10)
+    ref_x = np.array([float(s) for s in g["nodes"]])
+    ref_w = np.array([float(s) for s in g["weights"]])
+    # bit-for-bit: the reference table's decimal strings parse to the same doubles
+    assert np.array_equal(x, ref_x)
+    assert np.array_equal(w, ref_w)
+
+
+def test_bessel_against_mpmath(oracle_mod):
+    d = json.load(open(os.path.join(GOLDEN, "bessel_mpmath.json")))
+    worst = 0.0
+    for xi, x in enumerate(d["x"]):
+        J, Y = oracle_mod.bessel_jy(60, x)
+        Jr = np.array([float(s) for s in d["J"][xi]])
+        Yr = np.array([float(s) for s in d["Y"][xi]])
+        ok = np.abs(Jr) > 1e-290
+        ej = np.abs(J[ok] - Jr[ok]) / np.abs(Jr[ok])
+        ey = np.abs(Y - Yr) / np.abs(Yr)
+        worst = max(worst, ej.max(), ey.max())
+    assert worst < 1e-13, worst
+
+
+def _expected_child_lists(slots, parent_nb, parent_box):
+    """Lists of child c of parent_box from the reference's slot assignment."""
+    out = {}
+    for c in range(4):
+        nb = [-1] * 8
+        inner = [-1] * 16
+        outer = [-1] * 24
+        for e in slots:
+            if e["child"] != c:
+                continue
+            if e["parent_neighbor"] == -1:
+                val = 4 * parent_box + e["grandchild"]
+            else:
+                pn = parent_nb[e["parent_neighbor"]]
+                if pn == -1:
+                    continue
+                val = 4 * pn + e["grandchild"]
+            {"neighbor": nb, "inner": inner, "outer": outer}[e["kind"]][e["slot"]] = val
+        out[c] = (nb, inner, outer)
+    return out
+
+
+def test_interaction_lists_match_reference(oracle_mod, table_cache):
+    slots = json.load(open(os.path.join(GOLDEN, "interaction_slots.json")))["entries"]
+    p, (M, near, _) = table_cache(depth=4)
+    P = oracle_mod.Problem(p, M, near)
+    for j in range(0, 4):
+        for k in range(4 ** j):
+            pnb, _, _ = P.box_lists(j, k)
+            exp = _expected_child_lists(slots, list(pnb), k)
+            for c in range(4):
+                nb, inner, outer = P.box_lists(j + 1, 4 * k + c)
+                assert list(nb) == exp[c][0], (j, k, c)
+                assert list(inner) == exp[c][1], (j, k, c)
+                assert list(outer) == exp[c][2], (j, k, c)
+
+
+def test_near_and_far_entries_against_scipy_quadrature(oracle_mod, table_cache):
+    """An entry approximates (i/4) kappa^2 q(x_i) int_box H0(kappa|x_i-y|) phi_j(y) dy,
+    phi_j the least-squares polynomial of the source box (Q^+ row j)."""
+    from scipy import integrate, special
+    p, (M, near, qp) = table_cache(depth=3, kappa=10.0)
+    P = oracle_mod.Problem(p, M, near)
+    n = p.n_cheb
+    xy = P.grid_points()
+    q = P.contrast()
+    deg = p.degree
+    basis = [(a, d - a) for d in range(deg) for a in range(d + 1)]
+    r = 1.0 / 2 ** p.depth
+    leaf_c = xy.reshape(-1, n * n, 2).mean(axis=1)  # nodes are symmetric about the centre
+
+    def phi(jloc, u, v):
+        return sum(qp[l, jloc] * np.cos(a * np.arccos(u)) * np.cos(b * np.arccos(v))
+                   for l, (a, b) in enumerate(basis))
+
+    def direct(i, j):
+        lj, jloc = divmod(j, n * n)
+        cx, cy = leaf_c[lj]
+        xi = xy[i]
+
+        def f(v, u, part):
+            y0, y1 = cx + r * u, cy + r * v
+            R = p.kappa * np.hypot(xi[0] - y0, xi[1] - y1)
+            h = special.hankel1(0, R)
+            val = h * phi(jloc, u, v) * r * r
+            return val.real if part == 0 else val.imag
+        re = integrate.dblquad(f, -1, 1, -1, 1, args=(0,), epsabs=1e-11, epsrel=1e-10)[0]
+        im = integrate.dblquad(f, -1, 1, -1, 1, args=(1,), epsabs=1e-11, epsrel=1e-10)[0]
+        return 0.25j * (re + 1j * im) * p.kappa ** 2 * q[i]
+
+    # pick a target near the centre (large contrast); a far source two boxes away
+    # and an adjacent (near table) source
+    i = int(np.argmax(q))
+    li = i // (n * n)
+    cands = []
+    for lj in range(4 ** p.depth):
+        d = np.max(np.abs(leaf_c[lj] - leaf_c[li])) / (2 * r)
+        cands.append((round(d), lj))
+    far_leaf = [lj for d, lj in cands if d == 2][0]
+    near_leaf = [lj for d, lj in cands if d == 1][0]
+    for lj in (far_leaf, near_leaf):
+        j = lj * n * n + 7
+        got = P.entries([i], [j])[0]
+        ref = direct(i, j)
+        assert abs(got - ref) <= 2e-5 * abs(ref) + 1e-9, (lj, got, ref)
+
+
+def test_oracle_depth2_is_exact(oracle_mod, table_cache):
+    p, (M, near, _) = table_cache(depth=2, tol_pow=8)
+    P = oracle_mod.Problem(p, M, near)
+    b = P.rhs_plane_wave([0.0, 2.1])
+    x, _ = P.solve(b)
+    A = P.dense()
+    xd = np.linalg.solve(A, b.T).T
+    assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-12
+
+
+@pytest.mark.parametrize("q_kind", ["gauss_aw", "disk"])
+def test_oracle_elimination_solves_compressed_matrix(oracle_mod, table_cache, q_kind):
+    """With every fill-in recompressed (eliminate_phase) the elimination solves the
+    compressed matrix to the recompression tolerance; the driver's variant
+    (eliminate_phase_efficient) drops some fill-ins and lands further away."""
+    p, (M, near, _) = table_cache(depth=3, tol_pow=10, kappa=10.0)
+    p.q_kind = oracle_mod.Q_KINDS[q_kind]
+    P = oracle_mod.Problem(p, M, near)
+    At = P.compressed_dense()
+    b = P.rhs_plane_wave([0.0])
+    xt = np.linalg.solve(At, b[0])
+    P.set_variant(True)
+    x_full, _ = P.solve(b)
+    P2 = oracle_mod.Problem(p, M, near)
+    x_eff, _ = P2.solve(b)
+    assert np.linalg.norm(x_full[0] - xt) / np.linalg.norm(xt) < 1e-8
+    assert np.linalg.norm(x_eff[0] - xt) / np.linalg.norm(xt) < 1e-5
+    # the compressed matrix is close to the exact one in the sense of the solution
+    A = P.dense()
+    xd = np.linalg.solve(A, b[0])
+    assert np.linalg.norm(x_eff[0] - xd) / np.linalg.norm(xd) < 1e-3
