@@ -1,0 +1,275 @@
+"""aifmm_ls_b200 -- B200-native AIFMM direct solver for the 2-D Lippmann-Schwinger equation.
+
+Python face of the C ABI in include/aifmm_b200.h (libaifmm_b200.so, built
+in-tree for sm_100a).  The classes mirror the reference's surface:
+
+* ``LSKernel`` -- ``userkernel`` (kernel.hpp:90-193): grid points, the matrix
+  entries ``getMatrixEntry`` / ``getRow`` / ``getCol`` / ``getMatrix`` and the
+  leaf-level quadrature tables of LS/LS_Assembly.hpp.
+* ``FMM2DTree`` -- ``FMM2DTree<userkernel>`` (FMM2DTree_find_error.hpp): the
+  build / assemble / eliminate / back-substitute flow and ``error_check``.
+
+There is no CPU fallback: every call goes to the CUDA library and raises
+``AifmmError`` when it is missing or fails.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["AifmmError", "LSKernel", "FMM2DTree", "Desc", "load", "lib_path", "Q_KINDS"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "lib", "libaifmm_b200.so")
+_lib = None
+
+PTR_HOST, PTR_DEVICE, KEEP_ASSEMBLY = 0, 1, 2
+Q_KINDS = {"gaussian160": 0, "multi_gauss": 1, "plasma": 2, "flatbump": 3, "cavity": 4, "lens": 5,
+           "gauss_aw": 10, "disk": 11}
+
+
+class AifmmError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("aifmm status %d: %s" % (status, msg))
+        self.status = status
+
+
+class Desc(ctypes.Structure):
+    """aifmm_desc: the reference driver's argv (testFMM2D_find_error.cpp:44-52) plus contrast parameters."""
+    _fields_ = [("n_cheb", ctypes.c_int), ("kappa", ctypes.c_double), ("degree", ctypes.c_int),
+                ("L", ctypes.c_double), ("depth", ctypes.c_int), ("tol_pow", ctypes.c_int),
+                ("q_kind", ctypes.c_int), ("q_amp", ctypes.c_double), ("q_width", ctypes.c_double),
+                ("q_radius", ctypes.c_double)]
+
+
+# every entry point of include/aifmm_b200.h with its ctypes signature
+_P = ctypes.POINTER
+_d = _P(ctypes.c_double)
+_i = _P(ctypes.c_int)
+_v = ctypes.c_void_p
+SIGNATURES = {
+    "aifmm_problem_create": ([_P(Desc), ctypes.c_int, _P(_v)], ctypes.c_int),
+    "aifmm_problem_destroy": ([_v], ctypes.c_int),
+    "aifmm_last_error": ([_v], ctypes.c_char_p),
+    "aifmm_status_string": ([ctypes.c_int], ctypes.c_char_p),
+    "aifmm_tables_compute": ([_v, ctypes.c_int], ctypes.c_int),
+    "aifmm_tables_set": ([_v, _d, _d], ctypes.c_int),
+    "aifmm_tables_get": ([_v, _d, _d], ctypes.c_int),
+    "aifmm_num_points": ([_v, _i], ctypes.c_int),
+    "aifmm_grid_points": ([_v, _d], ctypes.c_int),
+    "aifmm_rhs_plane_wave": ([_v, ctypes.c_int, _d, _d, ctypes.c_int], ctypes.c_int),
+    "aifmm_entries": ([_v, ctypes.c_long, _i, _i, _d, ctypes.c_int], ctypes.c_int),
+    "aifmm_get_matrix": ([_v, ctypes.c_int, _i, ctypes.c_int, _i, _d, ctypes.c_int], ctypes.c_int),
+    "aifmm_build_tree": ([_v], ctypes.c_int),
+    "aifmm_assemble": ([_v], ctypes.c_int),
+    "aifmm_factorize_solve": ([_v, ctypes.c_int, _d, _d, ctypes.c_int], ctypes.c_int),
+    "aifmm_dense_matvec": ([_v, ctypes.c_int, _d, _d, ctypes.c_int], ctypes.c_int),
+    "aifmm_level_ranks": ([_v, ctypes.c_int, _i, _i], ctypes.c_int),
+    "aifmm_box_skeleton": ([_v, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i, ctypes.c_int, _i], ctypes.c_int),
+    "aifmm_phase_times": ([_v, _d], ctypes.c_int),
+    "aifmm_launch_counts": ([_v, _P(ctypes.c_long), _P(ctypes.c_long)], ctypes.c_int),
+    "aifmm_get_stream": ([_v, _P(_v)], ctypes.c_int),
+}
+
+
+def lib_path():
+    return _LIB
+
+
+def load():
+    """Load libaifmm_b200.so (building it first if the sources are newer)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            from . import build as _b
+            _b.build()
+        lib = ctypes.CDLL(_LIB)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(_d)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_i)
+
+
+def _c2r(a):
+    """complex128 array -> contiguous interleaved float64 view"""
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    return a.view(np.float64)
+
+
+class LSKernel:
+    """The Lippmann-Schwinger user kernel on one GPU (kernel.hpp userkernel + LS2DTree)."""
+
+    def __init__(self, n_cheb=6, kappa=10.0, degree=6, L=1.0, depth=5, tol_pow=8, q_kind="gaussian160",
+                 q_amp=1.5, q_width=32.0, q_radius=0.5, device=0):
+        lib = load()
+        k = Q_KINDS[q_kind] if isinstance(q_kind, str) else int(q_kind)
+        self.desc = Desc(n_cheb, float(kappa), degree, float(L), depth, tol_pow, k, float(q_amp),
+                         float(q_width), float(q_radius))
+        h = _v()
+        st = lib.aifmm_problem_create(ctypes.byref(self.desc), device, ctypes.byref(h))
+        if st != 0:
+            raise AifmmError(st, lib.aifmm_status_string(st).decode())
+        self.h = h
+        n = ctypes.c_int()
+        lib.aifmm_num_points(self.h, ctypes.byref(n))
+        self.N = n.value
+        self.rank = n_cheb * n_cheb
+        self.nLevelsResolve = depth
+
+    def _ck(self, st):
+        if st != 0:
+            raise AifmmError(st, load().aifmm_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().aifmm_problem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- precomputation (LS/LS_Assembly.hpp:270-276)
+    def tables_compute(self, round6=True):
+        self._ck(load().aifmm_tables_compute(self.h, 1 if round6 else 0))
+
+    def tables_set(self, M, near):
+        """M: 121 x rank complex; near: 9 x rank x rank complex (dir, i, j)."""
+        Mi = _c2r(np.asfortranarray(M).ravel(order="F"))
+        Ni = _c2r(np.concatenate([np.asarray(t).ravel(order="F") for t in near]))
+        self._ck(load().aifmm_tables_set(self.h, _dp(Mi), _dp(Ni)))
+
+    def tables_get(self):
+        r = self.rank
+        M = np.zeros(121 * r, dtype=np.complex128)
+        Nt = np.zeros(9 * r * r, dtype=np.complex128)
+        self._ck(load().aifmm_tables_get(self.h, _dp(M.view(np.float64)), _dp(Nt.view(np.float64))))
+        return M.reshape(121, r, order="F"), np.stack([Nt[d * r * r:(d + 1) * r * r].reshape(r, r, order="F")
+                                                       for d in range(9)])
+
+    # -- userkernel surface (kernel.hpp:49-86, 102-125)
+    @property
+    def gridPoints(self):
+        xy = np.zeros((self.N, 2))
+        self._ck(load().aifmm_grid_points(self.h, _dp(xy)))
+        return xy
+
+    def rhs_plane_wave(self, thetas):
+        th = np.ascontiguousarray(np.atleast_1d(thetas), dtype=np.float64)
+        b = np.zeros((len(th), self.N), dtype=np.complex128)
+        self._ck(load().aifmm_rhs_plane_wave(self.h, len(th), _dp(th), _dp(b.view(np.float64)), PTR_HOST))
+        return b
+
+    def entries(self, I, J):
+        I = np.ascontiguousarray(I, dtype=np.int32)
+        J = np.ascontiguousarray(J, dtype=np.int32)
+        out = np.zeros(len(I), dtype=np.complex128)
+        self._ck(load().aifmm_entries(self.h, len(I), _ip(I), _ip(J), _dp(out.view(np.float64)), PTR_HOST))
+        return out
+
+    def getMatrixEntry(self, i, j):
+        return self.entries([i], [j])[0]
+
+    def getMatrix(self, rows, cols):
+        rows = np.ascontiguousarray(rows, dtype=np.int32)
+        cols = np.ascontiguousarray(cols, dtype=np.int32)
+        out = np.zeros(len(rows) * len(cols), dtype=np.complex128)
+        self._ck(load().aifmm_get_matrix(self.h, len(rows), _ip(rows), len(cols), _ip(cols),
+                                         _dp(out.view(np.float64)), PTR_HOST))
+        return out.reshape(len(rows), len(cols), order="F")
+
+    def getRow(self, j, cols):
+        return self.getMatrix([j], cols)[0]
+
+    def getCol(self, k, rows):
+        return self.getMatrix(rows, [k])[:, 0]
+
+    def dense_matvec(self, x):
+        """y = A x with exact entries (the find_error fixture product); x: (nrhs, N)."""
+        x = np.atleast_2d(np.asarray(x, dtype=np.complex128))
+        xi = np.ascontiguousarray(x)
+        y = np.zeros_like(xi)
+        self._ck(load().aifmm_dense_matvec(self.h, x.shape[0], _dp(xi.view(np.float64)), _dp(y.view(np.float64)),
+                                           PTR_HOST))
+        return y
+
+
+class FMM2DTree:
+    """FMM2DTree<userkernel> (FMM2DTree_find_error.hpp) over an ``LSKernel``.
+
+    Method names follow the reference driver (testFMM2D_find_error.cpp:127-171).
+    """
+
+    def __init__(self, K, properties=None):
+        self.K = K
+        self.properties = None if properties is None else np.atleast_2d(np.asarray(properties, np.complex128))
+        self.x = None
+
+    def _ck(self, st):
+        self.K._ck(st)
+
+    # createTree + assign_Tree_Interactions (F:127-1070)
+    def createTree(self):
+        self._ck(load().aifmm_build_tree(self.K.h))
+
+    def assign_Tree_Interactions(self):
+        pass  # part of createTree on the device side
+
+    # assignLeafChargeLocations .. initialise_P2P_Leaf_Level (F:1072-1741)
+    def assemble(self):
+        self._ck(load().aifmm_assemble(self.K.h))
+
+    # eliminate_phase_efficient + back_substitution_phase with the rhs carried (F:2407-2532)
+    def solve(self, b=None, keep_assembly=False):
+        b = self.properties if b is None else np.atleast_2d(np.asarray(b, np.complex128))
+        if b is None:
+            raise ValueError("no right-hand side")
+        bi = np.ascontiguousarray(b)
+        x = np.zeros_like(bi)
+        flags = PTR_HOST | (KEEP_ASSEMBLY if keep_assembly else 0)
+        self._ck(load().aifmm_factorize_solve(self.K.h, b.shape[0], _dp(bi.view(np.float64)),
+                                              _dp(x.view(np.float64)), flags))
+        self.x = x
+        return x
+
+    def error_check(self, x_true):
+        """relative forward error ||x - x_true|| / ||x_true|| (F:2534-2581)"""
+        x_true = np.atleast_2d(x_true)
+        return float(np.linalg.norm(self.x - x_true) / np.linalg.norm(x_true))
+
+    def level_ranks(self, level):
+        n = 4 ** level
+        ri = np.zeros(n, dtype=np.int32)
+        ro = np.zeros(n, dtype=np.int32)
+        self._ck(load().aifmm_level_ranks(self.K.h, level, _ip(ri), _ip(ro)))
+        return ri, ro
+
+    def box_skeleton(self, level, box, which):
+        cap = 8192
+        out = np.zeros(cap, dtype=np.int32)
+        cnt = ctypes.c_int()
+        self._ck(load().aifmm_box_skeleton(self.K.h, level, box, which, _ip(out), cap, ctypes.byref(cnt)))
+        return out[:cnt.value].copy()
+
+    def phase_times(self):
+        ms = np.zeros(4)
+        self._ck(load().aifmm_phase_times(self.K.h, _dp(ms)))
+        return ms
+
+    def launch_counts(self):
+        a = ctypes.c_long()
+        b = ctypes.c_long()
+        self._ck(load().aifmm_launch_counts(self.K.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value

@@ -1,0 +1,64 @@
+// common.cuh -- shared device helpers for the AIFMM-LS B200 solver.
+//
+// Complex numbers are double2 (x = real, y = imaginary); matrices are
+// column-major with an explicit leading dimension.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cmath>
+
+#define AIFMM_HD __host__ __device__ __forceinline__
+
+AIFMM_HD double2 cmk(double re, double im) { return make_double2(re, im); }
+AIFMM_HD double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+AIFMM_HD double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+AIFMM_HD double2 cneg(double2 a) { return make_double2(-a.x, -a.y); }
+AIFMM_HD double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+AIFMM_HD double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+// (a+bi)(c+di) = (ac-bd) + (ad+bc)i
+AIFMM_HD double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+// conj(a) * b
+AIFMM_HD double2 cmulc(double2 a, double2 b) { return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x); }
+AIFMM_HD double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+AIFMM_HD double cabsd(double2 a) { return hypot(a.x, a.y); }
+// a / b (Smith's algorithm, as a compiler's complex division would do)
+AIFMM_HD double2 cdiv(double2 a, double2 b) {
+  if (fabs(b.x) >= fabs(b.y)) {
+    double r = b.y / b.x, d = b.x + b.y * r;
+    return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+  }
+  double r = b.x / b.y, d = b.x * r + b.y;
+  return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+}
+// c += a*b using fused multiply-adds
+AIFMM_HD double2 cfma(double2 a, double2 b, double2 c) {
+  c.x = fma(a.x, b.x, c.x); c.x = fma(-a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y); c.y = fma(a.y, b.x, c.y);
+  return c;
+}
+// c += conj(a)*b
+AIFMM_HD double2 cfmac(double2 a, double2 b, double2 c) {
+  c.x = fma(a.x, b.x, c.x); c.x = fma(a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y); c.y = fma(-a.y, b.x, c.y);
+  return c;
+}
+
+// Contrast kinds: 0..5 are the reference's Qchoice values (LS/LS_functions.hpp:99-112),
+// 10 = amp*exp(-width|x|^2), 11 = amp*[|x| < radius].
+enum { Q_GAUSSIAN160 = 0, Q_MULTI_GAUSS = 1, Q_PLASMA = 2, Q_FLATBUMP = 3, Q_CAVITY = 4,
+       Q_LENS = 5, Q_GAUSS_AW = 10, Q_DISK = 11 };
+
+// Everything a matrix-entry evaluation needs (all device pointers).
+struct EntryCtx {
+  int rank;        // points per leaf (n_cheb^2)
+  int depth;       // leaf level
+  double kappa;
+  const double2* pts;     // N grid points
+  const double* q;        // contrast at the grid points
+  const double2* leafc;   // leaf centres (Morton order)
+  const int2* leafxy;     // leaf grid coordinates
+  const double2* M;       // far-field coefficients, 121 x rank, column-major
+  const double2* nearT;   // 9 near tables, rank x rank column-major each
+};
+
+#define AIFMM_CUDA_OK(call) ((call) == cudaSuccess)

@@ -1,0 +1,461 @@
+// k_dense.cu -- batched small dense complex linear algebra for the bases and the
+// hierarchical elimination.
+//
+//  * Householder QR with column pivoting: the semantics of Eigen's
+//    ColPivHouseholderQR as used by FMM2DTree_find_error.hpp (:1535, :1819,
+//    :2092, :2477, :2493, :2510): pivot = first remaining column of largest
+//    (downdated) norm, LAPACK xGEQP3 norm downdating (LAPACK Working Note 176),
+//    reflector G = I - tau v v^H with beta = -sign(Re a_kk) |x|, exactly-nonzero
+//    pivot count from the eps-scaled initial column norm, rank() = #|R_ii| >
+//    threshold * max|R_ii|, solve() using only the nonzero pivots.
+//  * QR solves, explicit Q (householderQ().block(...)).
+//  * Partial-pivoting LU solves for the interpolative operators
+//    (get_L2P_P2M_box, :1105-1128).
+//  * Batched GEMM / GEAM / Frobenius norms.
+// One CTA per factorisation; everything else is batched over descriptor lists.
+#include <cfloat>
+#include "kernels.h"
+#include "entry.cuh"
+
+namespace {
+
+constexpr int kT = 256;
+constexpr int kW = kT / 32;
+constexpr double kPivotTie = 1e-11;  // same pivot tie tolerance as the ACA
+
+__device__ __forceinline__ double warp_sum(double x) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+__device__ __forceinline__ double2 warp_sum2(double2 x) {
+  for (int o = 16; o > 0; o >>= 1) {
+    x.x += __shfl_xor_sync(0xffffffffu, x.x, o);
+    x.y += __shfl_xor_sync(0xffffffffu, x.y, o);
+  }
+  return x;
+}
+
+__device__ double block_sum(double x, double* sh) {
+  x = warp_sum(x);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) { double r = 0; for (int w = 0; w < kW; ++w) r += sh[w]; sh[kW] = r; }
+  __syncthreads();
+  double r = sh[kW];
+  __syncthreads();
+  return r;
+}
+
+// ---------------------------------------------------------------- QR factor
+__global__ void __launch_bounds__(kT) qr_factor_kernel(const QRJob* __restrict__ jobs) {
+  const QRJob J = jobs[blockIdx.x];
+  __shared__ double sh[kW + 1];
+  __shared__ double sv[kW]; __shared__ int si[kW];
+  __shared__ double2 s_tau;
+  __shared__ int s_big;
+  const int m = J.m, n = J.n, size = min(m, n);
+  double2* A = J.a;
+  const int lda = J.lda;
+  double* nu = J.norms;
+  double* nd = J.norms + n;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int j = tid; j < n; j += kT) J.perm[j] = j;
+  // initial column norms (one warp per column)
+  for (int j = w; j < n; j += kW) {
+    double s = 0.0;
+    for (int i = lane; i < m; i += 32) s += cabs2(A[i + (size_t)j * lda]);
+    s = warp_sum(s);
+    if (lane == 0) { nu[j] = sqrt(s); nd[j] = nu[j]; }
+  }
+  __syncthreads();
+  double maxnorm = 0.0;
+  for (int j = 0; j < n; ++j) maxnorm = fmax(maxnorm, nu[j]);
+  const double eps = DBL_EPSILON;
+  const double thr_helper = m > 0 ? (maxnorm * eps) * (maxnorm * eps) / m : 0.0;
+  const double downdate_thr = sqrt(eps);
+  int nzp = size;
+  double maxpivot = 0.0;
+  for (int k = 0; k < size; ++k) {
+    // pivot: first largest updated norm among columns k..n-1
+    double bv = -1.0; int bi = -1;
+    for (int j = k + tid; j < n; j += kT) {
+      double v = nu[j];
+      if (bi < 0 || v > bv) { bv = v; bi = j; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double ov = __shfl_down_sync(0xffffffffu, bv, o);
+      int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (oi >= 0 && (bi < 0 || ov > bv || (ov == bv && oi < bi))) { bv = ov; bi = oi; }
+    }
+    if (lane == 0) { sv[w] = bv; si[w] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      double v = sv[0]; int i = si[0];
+      for (int q = 1; q < kW; ++q)
+        if (si[q] >= 0 && (i < 0 || sv[q] > v || (sv[q] == v && si[q] < i))) { v = sv[q]; i = si[q]; }
+      // norms within kPivotTie of the largest count as tied: first index wins
+      const double cut = v * (1.0 - kPivotTie);
+      for (int j = k; j < n; ++j)
+        if (nu[j] >= cut) { i = j; break; }
+      s_big = i;
+    }
+    __syncthreads();
+    const int big = s_big;
+    if (nzp == size && nu[big] * nu[big] < thr_helper * (double)(m - k)) nzp = k;
+    if (big != k) {
+      for (int i = tid; i < m; i += kT) {
+        double2 t = A[i + (size_t)k * lda];
+        A[i + (size_t)k * lda] = A[i + (size_t)big * lda];
+        A[i + (size_t)big * lda] = t;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        double t = nu[k]; nu[k] = nu[big]; nu[big] = t;
+        t = nd[k]; nd[k] = nd[big]; nd[big] = t;
+        int p = J.perm[k]; J.perm[k] = J.perm[big]; J.perm[big] = p;
+      }
+    }
+    // reflector for A(k:m, k)
+    double tail = 0.0;
+    for (int i = k + 1 + tid; i < m; i += kT) tail += cabs2(A[i + (size_t)k * lda]);
+    tail = block_sum(tail, sh);
+    const double2 c0 = A[k + (size_t)k * lda];
+    double beta;
+    if (tail <= DBL_MIN && c0.y * c0.y <= DBL_MIN) {
+      beta = c0.x;
+      if (tid == 0) { s_tau = make_double2(0.0, 0.0); }
+      for (int i = k + 1 + tid; i < m; i += kT) A[i + (size_t)k * lda] = make_double2(0.0, 0.0);
+    } else {
+      beta = sqrt(cabs2(c0) + tail);
+      if (c0.x >= 0.0) beta = -beta;
+      const double2 den = make_double2(c0.x - beta, c0.y);
+      if (tid == 0) {
+        s_tau = cconj(cdiv(make_double2(beta - c0.x, -c0.y), make_double2(beta, 0.0)));
+      }
+      for (int i = k + 1 + tid; i < m; i += kT) A[i + (size_t)k * lda] = cdiv(A[i + (size_t)k * lda], den);
+    }
+    __syncthreads();
+    const double2 t = s_tau;
+    if (tid == 0) { A[k + (size_t)k * lda] = make_double2(beta, 0.0); J.tau[k] = t; }
+    maxpivot = fmax(maxpivot, fabs(beta));
+    // apply G = I - t v v^H to columns k+1.. (one warp per column), then downdate norms
+    for (int j = k + 1 + w; j < n; j += kW) {
+      double2* col = A + (size_t)j * lda;
+      const double2* v = A + (size_t)k * lda;
+      double2 s = make_double2(0.0, 0.0);
+      for (int i = k + 1 + lane; i < m; i += 32) s = cfmac(v[i], col[i], s);
+      s = warp_sum2(s);
+      const double2 wv = cadd(col[k], s);
+      const double2 tw = cmul(t, wv);
+      for (int i = k + 1 + lane; i < m; i += 32) col[i] = csub(col[i], cmul(cmul(t, v[i]), wv));
+      __syncwarp();
+      if (lane == 0) col[k] = csub(col[k], tw);
+      __syncwarp();
+      // LAWN 176 downdate
+      double upd = nu[j];
+      if (upd != 0.0) {
+        double2 rkj = col[k];
+        double tmp = hypot(rkj.x, rkj.y) / upd;
+        tmp = (1.0 + tmp) * (1.0 - tmp);
+        if (tmp < 0.0) tmp = 0.0;
+        double rr = upd / nd[j];
+        double tmp2 = tmp * rr * rr;
+        if (tmp2 <= downdate_thr) {
+          double ss = 0.0;
+          for (int i = k + 1 + lane; i < m; i += 32) ss += cabs2(col[i]);
+          ss = warp_sum(ss);
+          if (lane == 0) { nd[j] = sqrt(ss); nu[j] = nd[j]; }
+        } else if (lane == 0) {
+          nu[j] = upd * sqrt(tmp);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const double thr = J.thr > 0.0 ? J.thr : (double)size * eps;
+    const double pre = fabs(maxpivot) * thr;
+    int rk = 0;
+    for (int i = 0; i < nzp; ++i) rk += (cabsd(A[i + (size_t)i * lda]) > pre);
+    J.info[0] = nzp;
+    J.info[1] = rk;
+    if (J.maxpiv) J.maxpiv[0] = maxpivot;
+  }
+}
+
+// ---------------------------------------------------------------- QR solve
+// one warp per right-hand side column
+__global__ void __launch_bounds__(kT) qr_solve_kernel(const SolveJob* __restrict__ jobs, const int* __restrict__ col_off,
+                                                      int njobs, int total_cols) {
+  const int gw = blockIdx.x * kW + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (gw >= total_cols) return;
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (col_off[mid] <= gw) lo = mid; else hi = mid - 1; }
+  const SolveJob J = jobs[lo];
+  const int c = gw - col_off[lo];
+  const int m = J.m, n = J.n;
+  const int nzp = J.info[0];
+  double2* x = J.X + (size_t)c * J.ldx;
+  if (nzp == 0) {
+    for (int i = lane; i < n; i += 32) x[i] = make_double2(0.0, 0.0);
+    return;
+  }
+  double2* wv = J.work + (size_t)c * m;
+  for (int i = lane; i < m; i += 32)
+    wv[i] = J.B ? J.B[i + (size_t)c * J.ldb] : make_double2(i == c ? 1.0 : 0.0, 0.0);
+  __syncwarp();
+  // Q^H b with the first nzp reflectors
+  for (int k = 0; k < nzp; ++k) {
+    const double2* v = J.qr + (size_t)k * J.ldq;
+    double2 s = make_double2(0.0, 0.0);
+    for (int i = k + 1 + lane; i < m; i += 32) s = cfmac(v[i], wv[i], s);
+    s = warp_sum2(s);
+    const double2 t = J.tau[k];
+    const double2 w = cadd(wv[k], s);
+    __syncwarp();
+    for (int i = k + 1 + lane; i < m; i += 32) wv[i] = csub(wv[i], cmul(cmul(t, v[i]), w));
+    if (lane == 0) wv[k] = csub(wv[k], cmul(t, w));
+    __syncwarp();
+  }
+  // back substitution with R(0:nzp, 0:nzp), column oriented
+  for (int i = nzp - 1; i >= 0; --i) {
+    double2 xi = cdiv(wv[i], J.qr[i + (size_t)i * J.ldq]);
+    __syncwarp();
+    if (lane == 0) wv[i] = xi;
+    for (int l = lane; l < i; l += 32) wv[l] = csub(wv[l], cmul(J.qr[l + (size_t)i * J.ldq], xi));
+    __syncwarp();
+  }
+  for (int i = lane; i < n; i += 32) x[i] = make_double2(0.0, 0.0);
+  __syncwarp();
+  for (int i = lane; i < nzp; i += 32) x[J.perm[i]] = cmul(J.alpha, wv[i]);
+}
+
+// ---------------------------------------------------------------- form Q
+__global__ void __launch_bounds__(kT) formq_kernel(const FormQJob* __restrict__ jobs, const int* __restrict__ col_off,
+                                                   int njobs, int total_cols) {
+  const int gw = blockIdx.x * kW + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (gw >= total_cols) return;
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (col_off[mid] <= gw) lo = mid; else hi = mid - 1; }
+  const FormQJob J = jobs[lo];
+  const int c = gw - col_off[lo];
+  const int ncols = J.ncols >= 0 ? J.ncols : J.ncols_dev[0];
+  if (c >= ncols) return;
+  const int m = J.m, size = min(J.m, J.n);
+  double2* q = J.Q + (size_t)c * J.ldQ;
+  for (int i = lane; i < m; i += 32) q[i] = make_double2(i == c ? 1.0 : 0.0, 0.0);
+  __syncwarp();
+  for (int k = min(size - 1, c); k >= 0; --k) {
+    const double2* v = J.qr + (size_t)k * J.ldq;
+    double2 s = make_double2(0.0, 0.0);
+    for (int i = k + 1 + lane; i < m; i += 32) s = cfmac(v[i], q[i], s);
+    s = warp_sum2(s);
+    const double2 t = cconj(J.tau[k]);
+    const double2 w = cadd(q[k], s);
+    __syncwarp();
+    for (int i = k + 1 + lane; i < m; i += 32) q[i] = csub(q[i], cmul(cmul(t, v[i]), w));
+    if (lane == 0) q[k] = csub(q[k], cmul(t, w));
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------- GEMM
+constexpr int TM = 32, TN = 32, TK = 16;
+__global__ void __launch_bounds__(256) gemm_kernel(const GemmDesc* __restrict__ ds, const GemmTerm* __restrict__ terms,
+                                                   const int* __restrict__ tile_off, int nd) {
+  const int bid = blockIdx.x;
+  int lo = 0, hi = nd - 1;
+  while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (tile_off[mid] <= bid) lo = mid; else hi = mid - 1; }
+  const GemmDesc D = ds[lo];
+  const int t = bid - tile_off[lo];
+  const int tiles_m = (D.m + TM - 1) / TM;
+  const int tm = t % tiles_m, tn = t / tiles_m;
+  __shared__ double2 As[TK][TM + 1];
+  __shared__ double2 Bs[TK][TN + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads, 2 x 2 outputs each
+  double2 acc[2][2];
+  for (int a = 0; a < 2; ++a) for (int b = 0; b < 2; ++b) acc[a][b] = make_double2(0.0, 0.0);
+  const int row0 = tm * TM, col0 = tn * TN;
+  for (int t_ = 0; t_ < D.nterms; ++t_) {
+  const GemmTerm T = terms[D.term0 + t_];
+  for (int k0 = 0; k0 < T.k; k0 += TK) {
+    for (int e = threadIdx.x; e < TK * TM; e += 256) {
+      int kk = e / TM, ii = e % TM;
+      int gi = row0 + ii, gk = k0 + kk;
+      double2 v = make_double2(0.0, 0.0);
+      if (gi < D.m && gk < T.k) v = T.opA ? cconj(T.A[gk + (size_t)gi * T.lda]) : T.A[gi + (size_t)gk * T.lda];
+      As[kk][ii] = v;
+    }
+    for (int e = threadIdx.x; e < TK * TN; e += 256) {
+      int jj = e / TK, kk = e % TK;
+      int gj = col0 + jj, gk = k0 + kk;
+      double2 v = make_double2(0.0, 0.0);
+      if (gj < D.n && gk < T.k) v = T.opB ? cconj(T.B[gj + (size_t)gk * T.ldb]) : T.B[gk + (size_t)gj * T.ldb];
+      Bs[kk][jj] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < TK; ++kk) {
+      double2 a0 = As[kk][ty], a1 = As[kk][ty + 16];
+      double2 b0 = Bs[kk][tx], b1 = Bs[kk][tx + 16];
+      acc[0][0] = cfma(a0, b0, acc[0][0]);
+      acc[0][1] = cfma(a0, b1, acc[0][1]);
+      acc[1][0] = cfma(a1, b0, acc[1][0]);
+      acc[1][1] = cfma(a1, b1, acc[1][1]);
+    }
+    __syncthreads();
+  }
+  }
+  const bool zero_beta = D.beta.x == 0.0 && D.beta.y == 0.0;
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b) {
+      int gi = row0 + ty + 16 * a, gj = col0 + tx + 16 * b;
+      if (gi < D.m && gj < D.n) {
+        double2* c = D.C + gi + (size_t)gj * D.ldc;
+        double2 v = cmul(D.alpha, acc[a][b]);
+        if (!zero_beta) v = cadd(v, cmul(D.beta, *c));
+        *c = v;
+      }
+    }
+}
+
+// ---------------------------------------------------------------- GEAM
+__global__ void geam_kernel(const GeamDesc* __restrict__ ds, const long long* __restrict__ off, int nd,
+                            long long total) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nd - 1;
+    while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (off[mid] <= e) lo = mid; else hi = mid - 1; }
+    const GeamDesc D = ds[lo];
+    long long loc = e - off[lo];
+    int i = (int)(loc % D.m), j = (int)(loc / D.m);
+    double2 a = D.opA ? cconj(D.A[j + (size_t)i * D.lda]) : D.A[i + (size_t)j * D.lda];
+    double2 v = cmul(D.alpha, a);
+    double2* c = D.C + i + (size_t)j * D.ldc;
+    if (!(D.beta.x == 0.0 && D.beta.y == 0.0)) v = cadd(v, cmul(D.beta, *c));
+    *c = v;
+  }
+}
+
+// ---------------------------------------------------------------- norms
+__global__ void __launch_bounds__(kT) norm_kernel(const NormDesc* __restrict__ ds) {
+  const NormDesc D = ds[blockIdx.x];
+  __shared__ double sh[kW + 1];
+  double s = 0.0;
+  for (long long e = threadIdx.x; e < (long long)D.m * D.n; e += kT) {
+    int i = (int)(e % D.m), j = (int)(e / D.m);
+    s += cabs2(D.A[i + (size_t)j * D.lda]);
+  }
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) D.out[0] = sqrt(s);
+}
+
+// ---------------------------------------------------------------- skeleton LU solve
+__global__ void __launch_bounds__(kT) skel_lu_kernel(const SkelLUJob* __restrict__ jobs, EntryCtx ctx) {
+  const SkelLUJob J = jobs[blockIdx.x];
+  const int r = J.r, m = J.m;
+  if (r == 0) return;
+  double2* D = J.work;             // r x r
+  double2* X = J.work + (size_t)r * r;  // r x m
+  const int tid = threadIdx.x;
+  __shared__ int s_p;
+  for (int e = tid; e < r * r; e += kT) {
+    int i = e % r, j = e / r;
+    if (J.adjD) D[i + (size_t)j * r] = cconj(lsa_entry(J.rows[j], J.cols[i], ctx));
+    else D[i + (size_t)j * r] = lsa_entry(J.rows[i], J.cols[j], ctx);
+  }
+  for (int e = tid; e < r * m; e += kT) {
+    int i = e % r, j = e / r;
+    X[i + (size_t)j * r] = J.adjB ? cconj(J.B[j + (size_t)i * J.ldb]) : J.B[i + (size_t)j * J.ldb];
+  }
+  __syncthreads();
+  // LU with partial pivoting (first row of largest modulus), row swaps applied to X
+  for (int k = 0; k < r; ++k) {
+    if (tid == 0) {
+      int p = k; double best = cabsd(D[k + (size_t)k * r]);
+      for (int i = k + 1; i < r; ++i) { double v = cabsd(D[i + (size_t)k * r]); if (v > best) { best = v; p = i; } }
+      s_p = p;
+      J.piv[k] = p;
+    }
+    __syncthreads();
+    const int p = s_p;
+    if (p != k) {
+      for (int j = tid; j < r; j += kT) { double2 t = D[k + (size_t)j * r]; D[k + (size_t)j * r] = D[p + (size_t)j * r]; D[p + (size_t)j * r] = t; }
+      for (int j = tid; j < m; j += kT) { double2 t = X[k + (size_t)j * r]; X[k + (size_t)j * r] = X[p + (size_t)j * r]; X[p + (size_t)j * r] = t; }
+    }
+    __syncthreads();
+    const double2 d = D[k + (size_t)k * r];
+    for (int i = k + 1 + tid; i < r; i += kT) {
+      if (!(d.x == 0.0 && d.y == 0.0)) D[i + (size_t)k * r] = cdiv(D[i + (size_t)k * r], d);
+    }
+    __syncthreads();
+    for (int e = tid; e < (r - k - 1) * (r - k - 1); e += kT) {
+      int i = k + 1 + e % (r - k - 1), j = k + 1 + e / (r - k - 1);
+      D[i + (size_t)j * r] = csub(D[i + (size_t)j * r], cmul(D[i + (size_t)k * r], D[k + (size_t)j * r]));
+    }
+    __syncthreads();
+  }
+  // forward (unit lower) and back substitution, one thread per right-hand side column
+  for (int j = tid; j < m; j += kT) {
+    double2* x = X + (size_t)j * r;
+    for (int i = 0; i < r; ++i) {
+      double2 s = x[i];
+      for (int l = 0; l < i; ++l) s = csub(s, cmul(D[i + (size_t)l * r], x[l]));
+      x[i] = s;
+    }
+    for (int i = r - 1; i >= 0; --i) {
+      double2 s = x[i];
+      for (int l = i + 1; l < r; ++l) s = csub(s, cmul(D[i + (size_t)l * r], x[l]));
+      x[i] = cdiv(s, D[i + (size_t)i * r]);
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < r * m; e += kT) {
+    int i = e % r, j = e / r;
+    if (J.adjX) J.X[j + (size_t)i * J.ldx] = cconj(X[i + (size_t)j * r]);
+    else J.X[i + (size_t)j * J.ldx] = X[i + (size_t)j * r];
+  }
+}
+
+}  // namespace
+
+int aifmm_launch_qr_factor(const QRJob* d_jobs, int njobs, cudaStream_t s) {
+  if (njobs <= 0) return 0;
+  qr_factor_kernel<<<njobs, kT, 0, s>>>(d_jobs);
+  return (int)cudaGetLastError();
+}
+int aifmm_launch_qr_solve(const SolveJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s) {
+  if (njobs <= 0 || total_cols <= 0) return 0;
+  qr_solve_kernel<<<(total_cols + kW - 1) / kW, kT, 0, s>>>(d_jobs, d_col_off, njobs, total_cols);
+  return (int)cudaGetLastError();
+}
+int aifmm_launch_formq(const FormQJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s) {
+  if (njobs <= 0 || total_cols <= 0) return 0;
+  formq_kernel<<<(total_cols + kW - 1) / kW, kT, 0, s>>>(d_jobs, d_col_off, njobs, total_cols);
+  return (int)cudaGetLastError();
+}
+int aifmm_launch_gemm(const GemmDesc* d, const GemmTerm* d_terms, const int* d_tile_off, int nd, int total_tiles,
+                      cudaStream_t s) {
+  if (nd <= 0 || total_tiles <= 0) return 0;
+  gemm_kernel<<<total_tiles, 256, 0, s>>>(d, d_terms, d_tile_off, nd);
+  return (int)cudaGetLastError();
+}
+int aifmm_launch_geam(const GeamDesc* d, const long long* d_off, int nd, long long total, cudaStream_t s) {
+  if (nd <= 0 || total <= 0) return 0;
+  long long blocks = (total + 255) / 256;
+  if (blocks > 148LL * 32) blocks = 148LL * 32;
+  geam_kernel<<<(int)blocks, 256, 0, s>>>(d, d_off, nd, total);
+  return (int)cudaGetLastError();
+}
+int aifmm_launch_norms(const NormDesc* d, int nd, cudaStream_t s) {
+  if (nd <= 0) return 0;
+  norm_kernel<<<nd, kT, 0, s>>>(d);
+  return (int)cudaGetLastError();
+}
+int aifmm_launch_skel_lu(const SkelLUJob* d, int nd, const EntryCtx& ctx, cudaStream_t s) {
+  if (nd <= 0) return 0;
+  skel_lu_kernel<<<nd, kT, 0, s>>>(d, ctx);
+  return (int)cudaGetLastError();
+}

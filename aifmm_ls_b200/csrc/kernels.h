@@ -1,0 +1,113 @@
+// kernels.h -- descriptor structs and launchers shared by the host orchestrator
+// and the CUDA kernels of the AIFMM-LS B200 solver.
+#pragma once
+#include "common.cuh"
+
+// ---- K1 entries
+struct BlockDesc {        // A(rows, cols) into out (column-major, ldo) or its adjoint
+  const int* rows;
+  const int* cols;
+  int nr, nc;
+  double2* out;
+  int ldo;
+  int adjoint;
+};
+
+// ---- K3 ACA
+struct AcaJob {
+  const int* rows;   // N1 global point indices
+  const int* cols;   // N2 global point indices
+  int n1, n2;
+  int want_rows;     // 1: keep unmodified rows (Ar, rank x N2, ld = rmax); 0: columns (Ac, N1 x rank, ld = N1)
+  double2* out;
+  double2* U;        // rmax x n_prim
+  double2* V;        // rmax x n_sec
+  double2* P;        // n_sec
+  double2* S;        // n_prim
+  double2* coef;     // rmax + 1
+  double2* dots_u;   // rmax + 1
+  double2* dots_v;   // rmax + 1
+  unsigned char* remP;
+  unsigned char* remS;
+  int* prim_bases;   // rmax
+  int* sec_bases;    // rmax
+  int* rank;         // [0] rank (-1: too large), [1] branch (1 rows first, 2 columns first)
+};
+
+// ---- dense
+struct QRJob {
+  double2* a; int lda;
+  int m, n;
+  double2* tau;
+  int* perm;
+  double* norms;     // 2n
+  double thr;        // 0 -> min(m,n)*eps
+  int* info;         // [0] nonzero pivots, [1] rank
+  double* maxpiv;
+};
+
+struct SolveJob {        // X = alpha * QR^{-1} B
+  const double2* qr; int ldq; int m, n;
+  const double2* tau; const int* perm; const int* info;
+  const double2* B; int ldb;   // nullptr -> identity
+  double2* X; int ldx;
+  int nrhs;
+  double2 alpha;
+  double2* work;         // m x nrhs
+};
+
+struct FormQJob {
+  const double2* qr; int ldq; int m, n;
+  const double2* tau;
+  double2* Q; int ldQ;
+  const int* ncols_dev;
+  int ncols;             // < 0 -> read ncols_dev[0]
+};
+
+struct GemmTerm {        // op(A) (m x k) * op(B) (k x n); op 0 = N, 1 = conjugate transpose
+  const double2* A; const double2* B;
+  int lda, ldb, opA, opB, k;
+};
+struct GemmDesc {        // C = alpha * sum_t op(A_t) op(B_t) + beta * C
+  double2* C; int ldc; int m, n;
+  double2 alpha, beta;
+  int term0, nterms;
+};
+
+struct GeamDesc {        // C = alpha op(A) + beta C
+  const double2* A; double2* C;
+  int lda, ldc, opA, m, n;
+  double2 alpha, beta;
+};
+
+struct NormDesc { const double2* A; int lda, m, n; double* out; };
+
+struct SkelLUJob {       // X = D^{-1} B, D = A(rows, cols) or its adjoint
+  const int* rows; const int* cols; int r;
+  int adjD;
+  const double2* B; int ldb; int adjB;
+  int m;
+  double2* X; int ldx; int adjX;
+  double2* work;         // r*r + r*m
+  int* piv;
+};
+
+// launchers (return a cudaError_t value)
+int aifmm_launch_tables(int n_cheb, int degree, double kappa, double r, const double* gl_x, const double* gl_w,
+                        const int2* basis, const double* cheb, double2* Cwork, double2* Vwork, int* status,
+                        double* qpinv, double2* M, double2* nearT, cudaStream_t stream);
+int aifmm_launch_block_entries(const BlockDesc* d_desc, const long long* d_off, int nd, long long total,
+                               const EntryCtx& ctx, cudaStream_t stream);
+int aifmm_launch_list_entries(const int* I, const int* J, long n, double2* out, const EntryCtx& ctx,
+                              cudaStream_t stream);
+int aifmm_launch_dense_matvec(const double2* x, double2* y, int N, int nrhs, const EntryCtx& ctx,
+                              cudaStream_t stream);
+int aifmm_launch_aca(const AcaJob* d_jobs, int njobs, double tol, const EntryCtx& ctx, cudaStream_t stream);
+int aifmm_launch_qr_factor(const QRJob* d_jobs, int njobs, cudaStream_t s);
+int aifmm_launch_qr_solve(const SolveJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s);
+int aifmm_launch_formq(const FormQJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s);
+int aifmm_launch_gemm(const GemmDesc* d, const GemmTerm* d_terms, const int* d_tile_off, int nd, int total_tiles,
+                      cudaStream_t s);
+int aifmm_launch_geam(const GeamDesc* d, const long long* d_off, int nd, long long total, cudaStream_t s);
+int aifmm_launch_norms(const NormDesc* d, int nd, cudaStream_t s);
+int aifmm_launch_skel_lu(const SkelLUJob* d, int nd, const EntryCtx& ctx, cudaStream_t s);

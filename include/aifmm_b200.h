@@ -1,0 +1,125 @@
+/*
+ * aifmm_b200.h -- C ABI of the B200 AIFMM-LS direct solver.
+ *
+ * A drop-in for the reference's (vaishna77/AIFMM_LS) solver path: the
+ * userkernel / LS2DTree matrix (kernel.hpp, LS/LS_Assembly.hpp) and the
+ * FMM2DTree build -> assemble -> eliminate -> back-substitute flow
+ * (FMM2DTree_find_error.hpp).  Every entry point below names the reference
+ * interface it replaces.  Plain C types only: complex numbers are interleaved
+ * (re, im) doubles, matrices are column-major, point sets are (x, y) pairs.
+ *
+ * Pointer arguments that carry bulk data accept either host or device memory,
+ * selected with AIFMM_PTR_DEVICE in `flags`; everything else is host memory.
+ * Calls on one handle must not overlap (one CUDA stream per handle); separate
+ * handles are independent.  Every call returns a status; aifmm_last_error()
+ * gives the message of the last failure on a handle.
+ */
+#ifndef AIFMM_B200_H
+#define AIFMM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AIFMM_ABI_VERSION 1
+
+typedef enum {
+  AIFMM_OK = 0,
+  AIFMM_ERR_ARG = 1,       /* invalid argument */
+  AIFMM_ERR_CUDA = 2,      /* CUDA runtime failure (message in aifmm_last_error) */
+  AIFMM_ERR_STATE = 3,     /* call out of order (e.g. solve before assemble) */
+  AIFMM_ERR_NOMEM = 4,     /* device allocation failed */
+  AIFMM_ERR_NUMERIC = 5,   /* inconsistent block shapes / quadrature budget exhausted */
+  AIFMM_ERR_NODEVICE = 6   /* no CUDA device */
+} aifmm_status;
+
+enum { AIFMM_PTR_HOST = 0, AIFMM_PTR_DEVICE = 1,
+       /* factorize_solve: keep a copy of the assembled blocks so that the handle can be
+        * solved again without re-assembling (the elimination consumes them otherwise) */
+       AIFMM_KEEP_ASSEMBLY = 2 };
+
+/* Contrast functions q(x): 0..5 are the reference's Qchoice values
+ * (LS/LS_functions.hpp:99-112: gaussian 1.5 exp(-160|x|^2), multipleGaussians,
+ * plasma, flatBump, cavity, lens); 10: amp*exp(-width*|x|^2); 11: amp*[|x| < radius]. */
+enum { AIFMM_Q_GAUSSIAN160 = 0, AIFMM_Q_MULTI_GAUSS = 1, AIFMM_Q_PLASMA = 2, AIFMM_Q_FLATBUMP = 3,
+       AIFMM_Q_CAVITY = 4, AIFMM_Q_LENS = 5, AIFMM_Q_GAUSS_AW = 10, AIFMM_Q_DISK = 11 };
+
+/* Problem description: the reference driver's argv
+ * (testFMM2D_find_error.cpp:44-52: nChebNodes kappa degreeOfBases L Qchoice TOL_POW nLevelsUniform)
+ * plus the parameters of the extra contrast kinds. */
+typedef struct {
+  int n_cheb;      /* Chebyshev nodes per leaf per dimension (nChebNodes) */
+  double kappa;    /* wavenumber */
+  int degree;      /* degreeOfBases: NB = degree*(degree+1)/2 polynomial bases */
+  double L;        /* half width of the domain */
+  int depth;       /* nLevelsUniform: leaf level of the uniform quadtree */
+  int tol_pow;     /* ACA and recompression tolerance 10^-tol_pow (TOL_POW) */
+  int q_kind;      /* contrast (see enum) */
+  double q_amp, q_width, q_radius;
+} aifmm_desc;
+
+typedef struct aifmm_problem aifmm_problem;
+
+/* Replaces userkernel(...) (kernel.hpp:106-128) -> LS2DTree(...) (LS/LS_Assembly.hpp:234-277)
+ * and FMM2DTree(...) (FMM2DTree_find_error.hpp:106-125): uniform tree, Chebyshev grid,
+ * contrast; binds a CUDA device.  The caller owns the handle. */
+aifmm_status aifmm_problem_create(const aifmm_desc* desc, int device, aifmm_problem** out);
+aifmm_status aifmm_problem_destroy(aifmm_problem* p);
+const char* aifmm_last_error(const aifmm_problem* p);
+const char* aifmm_status_string(aifmm_status s);
+
+/* Replaces evaluatePrecomputations / writeMToFile / getNeighborInteractions followed by
+ * readMFromFile / readNeighborInteractions (LS/LS_Assembly.hpp:270-276, 1166-1228, 1320-1459):
+ * leaf-level far-field coefficients M (121 x rank) and the 9 colleague near tables
+ * (rank x rank each), by adaptive Gauss-Legendre quadrature on the GPU.  round6 != 0
+ * applies the reference's text round trip (6 significant digits) to both. */
+aifmm_status aifmm_tables_compute(aifmm_problem* p, int round6);
+/* Supply / read the tables (host memory, interleaved complex, column-major:
+ * M is 121 x rank, near is 9 consecutive rank x rank tables). */
+aifmm_status aifmm_tables_set(aifmm_problem* p, const double* M, const double* near_tables);
+aifmm_status aifmm_tables_get(aifmm_problem* p, double* M, double* near_tables);
+
+/* userkernel::N (kernel.hpp:102) */
+aifmm_status aifmm_num_points(const aifmm_problem* p, int* n_points);
+/* userkernel::gridPoints (kernel.hpp:103; LS/LS_Assembly.hpp:1074-1087): N x 2 doubles (host) */
+aifmm_status aifmm_grid_points(aifmm_problem* p, double* xy);
+/* userKernel::RHSFunction (LS/LS_functions.hpp:113-120) for plane waves exp(i kappa (x cos t + y sin t)):
+ * b is N x nrhs complex; theta is host memory. */
+aifmm_status aifmm_rhs_plane_wave(aifmm_problem* p, int nrhs, const double* theta, double* b, int flags);
+
+/* userkernel::getMatrixEntry (kernel.hpp:130-136 -> LS/LS_Assembly.hpp:474-541) for n (I, J) pairs */
+aifmm_status aifmm_entries(aifmm_problem* p, long n, const int* I, const int* J, double* out, int flags);
+/* kernel::getMatrix (kernel.hpp:74-86): out is nr x nc complex, column-major (getRow / getCol are nr = 1 / nc = 1) */
+aifmm_status aifmm_get_matrix(aifmm_problem* p, int nr, const int* rows, int nc, const int* cols, double* out,
+                              int flags);
+
+/* FMM2DTree::createTree + assign_Tree_Interactions (FMM2DTree_find_error.hpp:127-1070) */
+aifmm_status aifmm_build_tree(aifmm_problem* p);
+/* FMM2DTree::assignLeafChargeLocations, getNodes (ACA skeletons, L2P/P2M), assemble_M2L,
+ * initialise_phase, initialise_P2P_Leaf_Level (FMM2DTree_find_error.hpp:1072-1361, 1714-1741) */
+aifmm_status aifmm_assemble(aifmm_problem* p);
+/* FMM2DTree::assign_Leaf_rhs, eliminate_phase_efficient, back_substitution_phase
+ * (FMM2DTree_find_error.hpp:1092-1103, 2407-2532) for nrhs right-hand sides at once:
+ * b and x are N x nrhs complex (column-major). */
+aifmm_status aifmm_factorize_solve(aifmm_problem* p, int nrhs, const double* b, double* x, int flags);
+
+/* The dense product of the find_error fixture generator (FMM2DTree_gen_rhs_x.hpp:2864-2871):
+ * y = A x with exact entries, x and y N x nrhs complex (nrhs <= 8). */
+aifmm_status aifmm_dense_matvec(aifmm_problem* p, int nrhs, const double* x, double* y, int flags);
+
+/* Introspection: ranks of the ACA skeletons of a level after assemble (incoming, outgoing,
+ * before the rank equalisation of get_L2P_P2M_box) and the skeleton point lists
+ * (which: 0 incoming check, 1 incoming charge, 2 outgoing check, 3 outgoing charge). */
+aifmm_status aifmm_level_ranks(aifmm_problem* p, int level, int* rank_in, int* rank_out);
+aifmm_status aifmm_box_skeleton(aifmm_problem* p, int level, int box, int which, int* out, int cap, int* count);
+/* Wall time of the last phases in ms: [0] build_tree [1] tables [2] assemble [3] factorize_solve. */
+aifmm_status aifmm_phase_times(const aifmm_problem* p, double* ms);
+/* Number of kernel launches issued by the last factorize_solve and by the last assemble. */
+aifmm_status aifmm_launch_counts(const aifmm_problem* p, long* factor_solve, long* assemble);
+/* The CUDA stream the handle works on (cudaStream_t). */
+aifmm_status aifmm_get_stream(const aifmm_problem* p, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AIFMM_B200_H */

@@ -42,6 +42,9 @@ namespace {
 using cd = std::complex<double>;
 const cd I1(0.0, 1.0);
 const double PI = 3.1415926535897932384;  // LSA:30
+// relative tolerance under which two pivot candidates (ACA entries, QR column
+// norms) are treated as equal; the first index then wins
+const double PIVOT_TIE = 1e-11;
 
 // --------------------------------------------------------------------------
 // Dense complex matrix (column-major), zero-initialised.
@@ -149,9 +152,11 @@ struct ColPivQR {
     nzp = size;
     maxpivot = 0.0;
     for (int k = 0; k < size; ++k) {
+      double mxn = 0.0;
+      for (int j = k; j < cols; ++j) mxn = std::max(mxn, nu[j]);
       int big = k;
-      for (int j = k + 1; j < cols; ++j)
-        if (nu[j] > nu[big]) big = j;
+      for (int j = k; j < cols; ++j)
+        if (nu[j] >= mxn * (1.0 - PIVOT_TIE)) { big = j; break; }
       double bigsq = nu[big] * nu[big];
       if (nzp == size && bigsq < thr_helper * (double)(rows - k)) nzp = k;
       if (big != k) {
@@ -683,6 +688,7 @@ struct Problem {
   double tol;
   std::vector<std::pair<int, int>> P2Pq, P2L_M2Pq;
   int nrhs = 1;
+  double perturb = 0.0;        // relative entry perturbation (sensitivity studies only)
   bool full_compress = false;  // eliminate_phase (F:2374) instead of the driver's _efficient
 
   static void box_xy(int k, int level, int& ix, int& iy) {
@@ -743,21 +749,31 @@ struct Problem {
     tol = std::pow(10, -1.0 * p.tol_pow);
   }
 
-  // LSA:474-541
   cd entry(int i, int j) const {
+    cd e = entry0(i, j);
+    if (perturb != 0.0) {
+      // deterministic pseudo-random relative perturbation in [-perturb, perturb]
+      unsigned long long h = (unsigned long long)i * 0x9E3779B97F4A7C15ull ^ ((unsigned long long)j + 0x632BE59BD9B4E019ull) * 0xBF58476D1CE4E5B9ull;
+      h ^= h >> 31; h *= 0x94D049BB133111EBull; h ^= h >> 29;
+      double u = (double)(h >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+      e *= (1.0 + perturb * u);
+    }
+    return e;
+  }
+  // LSA:474-541
+  cd entry0(int i, int j) const {
     const int li = i / rank, ii = i % rank, lj = j / rank, jj = j % rank;
     int xi, yi, xj, yj;
     box_xy(li, depth, xi, yi);
     box_xy(lj, depth, xj, yj);
     int dx = xj - xi, dy = yj - yi;
     const P2 ri = pts[i];
-    const double kq = p.kappa * p.kappa * q[i];
     if (std::abs(dx) <= 1 && std::abs(dy) <= 1) {
       int dir = 8;
       for (int d = 0; d < 8; ++d)
         if (NB_DX[d] == dx && NB_DY[d] == dy) dir = d;
       cd e = T.near[(size_t)dir * rank * rank + ii + (size_t)jj * rank];
-      e = e * kq;
+      e = e * p.kappa * p.kappa * q[i];  // LSA:508, evaluated left to right
       if (i == j) e = 1.0 + e;
       if (std::abs(e) < 1e-16) e = 0.0;
       return e;
@@ -780,7 +796,7 @@ struct Problem {
       s += Mc[n + 60] * t;
     }
     s *= I1 / 4.0;
-    s *= kq;
+    s *= p.kappa * p.kappa * q[i];  // LSA:531
     if (i == j) s += 1.0;
     if (std::abs(s) < 1e-16) s = 0.0;
     return s;
@@ -856,13 +872,17 @@ struct Problem {
 
   // ---------------- ACA (ACA.hpp:368-577) ----------------
   static void maxAbs(const std::vector<cd>& v, const std::set<int>& allowed, int& index) {
-    // ACA.hpp:27-40: first maximum of |v| over allowed indices in ascending order
+    // ACA.hpp:27-40: first maximum of |v| over allowed indices in ascending order.
+    // Magnitudes within PIVOT_TIE (relative) of the maximum count as tied, so that
+    // mathematically equal candidates (mirror-symmetric grids and contrasts) are
+    // resolved by index rather than by rounding noise.
     if (allowed.empty()) { index = 0; return; }
-    auto it = allowed.begin();
-    index = *it;
-    double mx = std::abs(v[index]);
-    for (; it != allowed.end(); ++it)
-      if (std::abs(v[*it]) > mx) { index = *it; mx = std::abs(v[*it]); }
+    double mx = 0.0;
+    for (int i : allowed) mx = std::max(mx, std::abs(v[i]));
+    const double cut = mx * (1.0 - PIVOT_TIE);
+    for (int i : allowed)
+      if (std::abs(v[i]) >= cut) { index = i; return; }
+    index = *allowed.begin();
   }
   static cd dotc(const std::vector<cd>& a, const std::vector<cd>& b) {
     cd s(0, 0);
@@ -1740,6 +1760,11 @@ void* orc_create(const orc_params* p, const double* M, const double* near_tab) {
 void orc_destroy(void* h) { delete static_cast<Problem*>(h); }
 
 int orc_num_points(void* h) { return static_cast<Problem*>(h)->N; }
+
+int orc_set_perturbation(void* h, double rel) {
+  static_cast<Problem*>(h)->perturb = rel;
+  return 0;
+}
 
 int orc_set_variant(void* h, int full_compress) {
   static_cast<Problem*>(h)->full_compress = full_compress != 0;

@@ -69,6 +69,10 @@ int orc_dense_matvec(void* h, int nrhs, const double* x, double* y);
 /* Full pipeline: assemble, eliminate_phase_efficient (with the rhs carried),
  * base solve, back substitution.  times[4] = tree, assemble, factor, solve (s). */
 int orc_solve(void* h, int nrhs, const double* b, double* x, double* times);
+/* Multiply every matrix entry by (1 + rel*u), u a fixed pseudo-random number in
+ * [-1, 1] per (i, j): used to measure how strongly the algorithm amplifies
+ * last-bit differences in the entries. */
+int orc_set_perturbation(void* h, double rel);
 /* 0: eliminate_phase_efficient (the reference driver's choice, default);
  * 1: eliminate_phase (compress every queued pair after each box). */
 int orc_set_variant(void* h, int full_compress);

@@ -56,6 +56,7 @@ def lib():
         _lib.orc_dense_matvec.argtypes = [v, ctypes.c_int, d, d]
         _lib.orc_solve.argtypes = [v, ctypes.c_int, d, d, d]
         _lib.orc_set_variant.argtypes = [v, ctypes.c_int]
+        _lib.orc_set_perturbation.argtypes = [v, ctypes.c_double]
         _lib.orc_compressed_dense.argtypes = [P(OrcParams), d, d, d]
         _lib.orc_level_ranks.argtypes = [v, ctypes.c_int, i, i]
         _lib.orc_box_lists.argtypes = [v, ctypes.c_int, ctypes.c_int, i]
@@ -128,6 +129,9 @@ class Problem:
 
     def set_variant(self, full_compress):
         lib().orc_set_variant(self.h, 1 if full_compress else 0)
+
+    def set_perturbation(self, rel):
+        lib().orc_set_perturbation(self.h, float(rel))
 
     def compressed_dense(self):
         """Dense matrix implied by the pre-elimination compressed representation."""

@@ -1,0 +1,59 @@
+"""CPU checks of the product library: it builds for sm_100a, loads, exports every
+entry point declared in include/aifmm_b200.h, and refuses to run without a GPU
+(there is no CPU fallback)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    src = open(os.path.join(ROOT, "include", "aifmm_b200.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\*?\s+\*?(aifmm_\w+)\s*\(", src, re.M)))
+
+
+def test_header_declares_the_abi():
+    syms = _declared_symbols()
+    assert "aifmm_problem_create" in syms and "aifmm_factorize_solve" in syms
+    assert len(syms) >= 20
+
+
+def test_library_builds_and_exports_every_declared_symbol():
+    import aifmm_ls_b200 as A
+    from aifmm_ls_b200 import build
+    path = build.build()
+    assert os.path.exists(path)
+    lib = ctypes.CDLL(path)
+    missing = [s for s in _declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    # the Python binding covers the same set
+    assert set(_declared_symbols()) == set(A.SIGNATURES)
+
+
+def test_status_strings():
+    import aifmm_ls_b200 as A
+    lib = A.load()
+    for s in range(7):
+        assert lib.aifmm_status_string(s)
+
+
+def test_no_cpu_fallback_without_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import aifmm_ls_b200 as A
+    with pytest.raises(A.AifmmError) as e:
+        A.LSKernel(depth=2)
+    assert e.value.status in (2, 6)  # CUDA error / no device
+
+
+def test_invalid_description_is_rejected():
+    import aifmm_ls_b200 as A
+    lib = A.load()
+    d = A.Desc(6, 10.0, 6, 1.0, 1, 8, 0, 1.5, 32.0, 0.5)  # depth 1 is not a valid AIFMM tree
+    h = ctypes.c_void_p()
+    st = lib.aifmm_problem_create(ctypes.byref(d), 0, ctypes.byref(h))
+    assert st != 0
