@@ -69,6 +69,7 @@ SIGNATURES = {
     "aifmm_phase_times": ([_v, _d], ctypes.c_int),
     "aifmm_launch_counts": ([_v, _P(ctypes.c_long), _P(ctypes.c_long)], ctypes.c_int),
     "aifmm_get_stream": ([_v, _P(_v)], ctypes.c_int),
+    "aifmm_stats": ([_v, _d, ctypes.c_int], ctypes.c_int),
 }
 
 
@@ -267,6 +268,12 @@ class FMM2DTree:
         ms = np.zeros(4)
         self._ck(load().aifmm_phase_times(self.K.h, _dp(ms)))
         return ms
+
+    def stats(self):
+        v = np.zeros(8)
+        self._ck(load().aifmm_stats(self.K.h, _dp(v), 8))
+        keys = ["sync_ms", "syncs", "pending_ms", "elim_ms", "back_ms", "compressions", "total_ms", "launches"]
+        return dict(zip(keys, v.tolist()))
 
     def launch_counts(self):
         a = ctypes.c_long()

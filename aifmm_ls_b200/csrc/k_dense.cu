@@ -47,19 +47,16 @@ __device__ double block_sum(double x, double* sh) {
 }
 
 // ---------------------------------------------------------------- QR factor
-__global__ void __launch_bounds__(kT) qr_factor_kernel(const QRJob* __restrict__ jobs) {
-  const QRJob J = jobs[blockIdx.x];
+// The factorisation runs on A (lda), nu/nd (norm arrays) and perm, either in
+// global memory or staged in shared memory (qr_factor_smem_kernel).
+__device__ void qr_factor_body(const QRJob& J, double2* A, int lda, double* nu, double* nd, int* perm) {
   __shared__ double sh[kW + 1];
   __shared__ double sv[kW]; __shared__ int si[kW];
   __shared__ double2 s_tau;
   __shared__ int s_big;
   const int m = J.m, n = J.n, size = min(m, n);
-  double2* A = J.a;
-  const int lda = J.lda;
-  double* nu = J.norms;
-  double* nd = J.norms + n;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  for (int j = tid; j < n; j += kT) J.perm[j] = j;
+  for (int j = tid; j < n; j += kT) perm[j] = j;
   // initial column norms (one warp per column)
   for (int j = w; j < n; j += kW) {
     double s = 0.0;
@@ -112,7 +109,7 @@ __global__ void __launch_bounds__(kT) qr_factor_kernel(const QRJob* __restrict__
       if (tid == 0) {
         double t = nu[k]; nu[k] = nu[big]; nu[big] = t;
         t = nd[k]; nd[k] = nd[big]; nd[big] = t;
-        int p = J.perm[k]; J.perm[k] = J.perm[big]; J.perm[big] = p;
+        int p = perm[k]; perm[k] = perm[big]; perm[big] = p;
       }
     }
     // reflector for A(k:m, k)
@@ -180,6 +177,243 @@ __global__ void __launch_bounds__(kT) qr_factor_kernel(const QRJob* __restrict__
     J.info[0] = nzp;
     J.info[1] = rk;
     if (J.maxpiv) J.maxpiv[0] = maxpivot;
+  }
+}
+
+__global__ void __launch_bounds__(kT) qr_factor_kernel(const QRJob* __restrict__ jobs) {
+  const QRJob J = jobs[blockIdx.x];
+  qr_factor_body(J, J.a, J.lda, J.norms, J.norms + J.n, J.perm);
+}
+
+// Jobs whose matrix fits in shared memory.  Each thread owns whole columns
+// (j = tid, tid + kT, ...): dot products, updates and norm downdates run down
+// its own columns without reductions; warp 0 builds the reflector; three
+// barriers per pivot step.  Same arithmetic order per column as the oracle.
+__global__ void __launch_bounds__(kT) qr_factor_smem_kernel(const QRJob* __restrict__ jobs) {
+  extern __shared__ double2 smem[];
+  __shared__ int s_big;
+  __shared__ double2 s_tau;
+  __shared__ double s_beta;
+  const QRJob J = jobs[blockIdx.x];
+  const int m = J.m, n = J.n, size = min(m, n);
+  const int tid = threadIdx.x, lane = tid & 31;
+  // odd leading dimension: threads walking their own columns hit distinct banks
+  const int ld = m | 1;
+  double2* A = smem;  // m x n
+  double* nu = reinterpret_cast<double*>(A + (size_t)ld * n);
+  double* nd = nu + n;
+  int* perm = reinterpret_cast<int*>(nd + n);
+  for (int e = tid; e < m * n; e += kT) {
+    const int i = e % m, j = e / m;
+    A[i + (size_t)j * ld] = J.a[i + (size_t)j * J.lda];
+  }
+  for (int j = tid; j < n; j += kT) perm[j] = j;
+  __syncthreads();
+  for (int j = tid; j < n; j += kT) {
+    double sq = 0.0;
+    const double2* col = A + (size_t)j * ld;
+    for (int i = 0; i < m; ++i) sq += cabs2(col[i]);
+    nu[j] = sqrt(sq);
+    nd[j] = nu[j];
+  }
+  __syncthreads();
+  double maxnorm = 0.0;
+  for (int j = 0; j < n; ++j) maxnorm = fmax(maxnorm, nu[j]);
+  const double eps = DBL_EPSILON;
+  const double thr_helper = m > 0 ? (maxnorm * eps) * (maxnorm * eps) / m : 0.0;
+  const double downdate_thr = sqrt(eps);
+  int nzp = size;
+  double maxpivot = 0.0;
+  for (int k = 0; k < size; ++k) {
+    // pivot (warp 0): largest norm among k..n-1, first index within the tie tolerance
+    if (tid < 32) {
+      double mx = 0.0;
+      for (int j = k + lane; j < n; j += 32) mx = fmax(mx, nu[j]);
+      for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      const double cut = mx * (1.0 - kPivotTie);
+      int first = 0x7fffffff;
+      for (int j = k + lane; j < n; j += 32) if (nu[j] >= cut) { first = j; break; }
+      for (int o = 16; o > 0; o >>= 1) first = min(first, __shfl_xor_sync(0xffffffffu, first, o));
+      if (lane == 0) s_big = first >= n ? k : first;
+    }
+    __syncthreads();
+    const int big = s_big;
+    if (nzp == size && nu[big] * nu[big] < thr_helper * (double)(m - k)) nzp = k;
+    // swap columns k and big (warp 0), then the reflector for A(k:m, k) (warp 0)
+    if (tid < 32) {
+      if (big != k) {
+        for (int i = lane; i < m; i += 32) {
+          double2 t = A[i + (size_t)k * ld];
+          A[i + (size_t)k * ld] = A[i + (size_t)big * ld];
+          A[i + (size_t)big * ld] = t;
+        }
+        if (lane == 0) {
+          double t = nu[k]; nu[k] = nu[big]; nu[big] = t;
+          t = nd[k]; nd[k] = nd[big]; nd[big] = t;
+          int p = perm[k]; perm[k] = perm[big]; perm[big] = p;
+        }
+        __syncwarp();
+      }
+      double tail = 0.0;
+      for (int i = k + 1 + lane; i < m; i += 32) tail += cabs2(A[i + (size_t)k * ld]);
+      tail = warp_sum(tail);
+      const double2 c0 = A[k + (size_t)k * ld];
+      double beta;
+      double2 t;
+      if (tail <= DBL_MIN && c0.y * c0.y <= DBL_MIN) {
+        beta = c0.x;
+        t = make_double2(0.0, 0.0);
+        for (int i = k + 1 + lane; i < m; i += 32) A[i + (size_t)k * ld] = make_double2(0.0, 0.0);
+      } else {
+        beta = sqrt(cabs2(c0) + tail);
+        if (c0.x >= 0.0) beta = -beta;
+        const double2 den = make_double2(c0.x - beta, c0.y);
+        t = cconj(cdiv(make_double2(beta - c0.x, -c0.y), make_double2(beta, 0.0)));
+        for (int i = k + 1 + lane; i < m; i += 32) A[i + (size_t)k * ld] = cdiv(A[i + (size_t)k * ld], den);
+      }
+      __syncwarp();
+      if (lane == 0) { A[k + (size_t)k * ld] = make_double2(beta, 0.0); s_tau = t; s_beta = beta; J.tau[k] = t; }
+    }
+    __syncthreads();
+    const double2 t = s_tau;
+    maxpivot = fmax(maxpivot, fabs(s_beta));
+    // apply G = I - t v v^H to the columns this thread owns, then downdate their norms
+    const double2* v = A + (size_t)k * ld;
+    for (int j = k + 1 + tid; j < n; j += kT) {
+      double2* col = A + (size_t)j * ld;
+      double2 s0 = make_double2(0.0, 0.0), s1 = make_double2(0.0, 0.0);
+      int i = k + 1;
+      for (; i + 1 < m; i += 2) { s0 = cfmac(v[i], col[i], s0); s1 = cfmac(v[i + 1], col[i + 1], s1); }
+      if (i < m) s0 = cfmac(v[i], col[i], s0);
+      const double2 wv = cadd(col[k], cadd(s0, s1));
+      for (int r = k + 1; r < m; ++r) col[r] = csub(col[r], cmul(cmul(t, v[r]), wv));
+      col[k] = csub(col[k], cmul(t, wv));
+      const double upd = nu[j];
+      if (upd != 0.0) {
+        double tmp = cabsd(col[k]) / upd;
+        tmp = (1.0 + tmp) * (1.0 - tmp);
+        if (tmp < 0.0) tmp = 0.0;
+        const double rr = upd / nd[j];
+        const double tmp2 = tmp * rr * rr;
+        if (tmp2 <= downdate_thr) {
+          double ss = 0.0;
+          for (int r = k + 1; r < m; ++r) ss += cabs2(col[r]);
+          nd[j] = sqrt(ss);
+          nu[j] = nd[j];
+        } else {
+          nu[j] = upd * sqrt(tmp);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < m * n; e += kT) {
+    const int i = e % m, j = e / m;
+    J.a[i + (size_t)j * J.lda] = A[i + (size_t)j * ld];
+  }
+  for (int j = tid; j < n; j += kT) J.perm[j] = perm[j];
+  if (tid == 0) {
+    const double thr = J.thr > 0.0 ? J.thr : (double)size * eps;
+    const double pre = fabs(maxpivot) * thr;
+    int rk = 0;
+    for (int i = 0; i < nzp; ++i) rk += (cabsd(A[i + (size_t)i * ld]) > pre);
+    J.info[0] = nzp;
+    J.info[1] = rk;
+    if (J.maxpiv) J.maxpiv[0] = maxpivot;
+  }
+}
+
+// ---------------------------------------------------------------- QR solve (panel in shared memory)
+// One CTA per (job, panel of kSolveCols right-hand sides).  The panel B (m x
+// kSolveCols) and, when it fits, the first nzp columns of the factor live in
+// shared memory.  For each reflector, 4 threads per column form v^H b and all
+// threads apply the rank-1 update; back substitution is column oriented.
+constexpr int kSolveCols = 64;
+__global__ void __launch_bounds__(kT) qr_solve_cols_kernel(const SolveJob* __restrict__ jobs,
+                                                           const int* __restrict__ cta_off, int njobs,
+                                                           int smem_cols_cap) {
+  extern __shared__ double2 fs[];
+  __shared__ double2 wdot[kSolveCols];
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cta_off[mid] <= (int)blockIdx.x) lo = mid; else hi = mid - 1; }
+  const SolveJob J = jobs[lo];
+  const int chunk = blockIdx.x - cta_off[lo];
+  const int m = J.m, n = J.n;
+  const int nzp = J.info[0];
+  const int c0 = chunk * kSolveCols;
+  const int nc = min(kSolveCols, J.nrhs - c0);
+  const int tid = threadIdx.x;
+  if (nzp == 0) {
+    for (int e = tid; e < n * nc; e += kT) {
+      const int i = e % n, c = e / n;
+      J.X[i + (size_t)(c0 + c) * J.ldx] = make_double2(0.0, 0.0);
+    }
+    return;
+  }
+  const bool fac_in_smem = nzp <= smem_cols_cap;
+  const int ldb = m | 1;                             // odd: column-wise accesses spread over banks
+  double2* B = fs;                                   // m x kSolveCols
+  double2* F = fs + (size_t)ldb * kSolveCols;        // m x nzp
+  double2* tauS = F + (size_t)m * (fac_in_smem ? nzp : 0);
+  for (int e = tid; e < m * nc; e += kT) {
+    const int i = e % m, c = e / m;
+    B[i + (size_t)c * ldb] = J.B ? J.B[i + (size_t)(c0 + c) * J.ldb] : make_double2(i == c0 + c ? 1.0 : 0.0, 0.0);
+  }
+  if (fac_in_smem) {
+    for (int e = tid; e < m * nzp; e += kT) {
+      const int i = e % m, j = e / m;
+      F[e] = J.qr[i + (size_t)j * J.ldq];
+    }
+    for (int k = tid; k < nzp; k += kT) tauS[k] = J.tau[k];
+  }
+  __syncthreads();
+  const double2* Q = fac_in_smem ? F : J.qr;
+  const int ldq = fac_in_smem ? m : J.ldq;
+  const double2* T = fac_in_smem ? tauS : J.tau;
+  const int c = tid >> 2, part = tid & 3;  // 4 threads per column for the dots
+  for (int k = 0; k < nzp; ++k) {
+    const double2* v = Q + (size_t)k * ldq;
+    if (c < nc) {
+      const double2* col = B + (size_t)c * ldb;
+      double2 s = make_double2(0.0, 0.0);
+      for (int i = k + 1 + part; i < m; i += 4) s = cfmac(v[i], col[i], s);
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, 1); s.y += __shfl_xor_sync(0xffffffffu, s.y, 1);
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, 2); s.y += __shfl_xor_sync(0xffffffffu, s.y, 2);
+      if (part == 0) wdot[c] = cmul(T[k], cadd(col[k], s));  // t * (v^H b)
+    } else {
+      // keep the shuffles of the warp converged
+      double2 s = make_double2(0.0, 0.0);
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, 1); s.y += __shfl_xor_sync(0xffffffffu, s.y, 1);
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, 2); s.y += __shfl_xor_sync(0xffffffffu, s.y, 2);
+    }
+    __syncthreads();
+    for (int e = tid; e < (m - k) * nc; e += kT) {
+      const int i = k + e % (m - k), cc = e / (m - k);
+      const double2 tw = wdot[cc];
+      double2* bb = B + i + (size_t)cc * ldb;
+      if (i == k) *bb = csub(*bb, tw);
+      else *bb = csub(*bb, cmul(v[i], tw));
+    }
+    __syncthreads();
+  }
+  for (int i = nzp - 1; i >= 0; --i) {
+    const double2 rii = Q[i + (size_t)i * ldq];
+    for (int cc = tid; cc < nc; cc += kT) B[i + (size_t)cc * ldb] = cdiv(B[i + (size_t)cc * ldb], rii);
+    __syncthreads();
+    for (int e = tid; e < i * nc; e += kT) {
+      const int l = e % i, cc = e / i;
+      B[l + (size_t)cc * ldb] = csub(B[l + (size_t)cc * ldb], cmul(Q[l + (size_t)i * ldq], B[i + (size_t)cc * ldb]));
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < n * nc; e += kT) {
+    const int i = e % n, cc = e / n;
+    J.X[i + (size_t)(c0 + cc) * J.ldx] = make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  for (int e = tid; e < nzp * nc; e += kT) {
+    const int i = e % nzp, cc = e / nzp;
+    J.X[J.perm[i] + (size_t)(c0 + cc) * J.ldx] = cmul(J.alpha, B[i + (size_t)cc * ldb]);
   }
 }
 
@@ -424,6 +658,30 @@ __global__ void __launch_bounds__(kT) skel_lu_kernel(const SkelLUJob* __restrict
 int aifmm_launch_qr_factor(const QRJob* d_jobs, int njobs, cudaStream_t s) {
   if (njobs <= 0) return 0;
   qr_factor_kernel<<<njobs, kT, 0, s>>>(d_jobs);
+  return (int)cudaGetLastError();
+}
+size_t aifmm_qr_smem_bytes(int m, int n) {
+  return sizeof(double2) * (size_t)(m | 1) * n + sizeof(double) * 2 * (size_t)n + sizeof(int) * (size_t)n + 64;
+}
+int aifmm_launch_qr_factor_smem(const QRJob* d_jobs, int njobs, size_t smem, cudaStream_t s) {
+  if (njobs <= 0) return 0;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(qr_factor_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    attr = true;
+  }
+  qr_factor_smem_kernel<<<njobs, kT, smem, s>>>(d_jobs);
+  return (int)cudaGetLastError();
+}
+int aifmm_launch_qr_solve_cols(const SolveJob* d_jobs, const int* d_cta_off, int njobs, int total_ctas,
+                               int smem_cols_cap, size_t smem, cudaStream_t s) {
+  if (njobs <= 0 || total_ctas <= 0) return 0;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(qr_solve_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    attr = true;
+  }
+  qr_solve_cols_kernel<<<total_ctas, kT, smem, s>>>(d_jobs, d_cta_off, njobs, smem_cols_cap);
   return (int)cudaGetLastError();
 }
 int aifmm_launch_qr_solve(const SolveJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s) {

@@ -105,6 +105,12 @@ int aifmm_launch_dense_matvec(const double2* x, double2* y, int N, int nrhs, con
 int aifmm_launch_aca(const AcaJob* d_jobs, int njobs, double tol, const EntryCtx& ctx, cudaStream_t stream);
 int aifmm_launch_qr_factor(const QRJob* d_jobs, int njobs, cudaStream_t s);
 int aifmm_launch_qr_solve(const SolveJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s);
+size_t aifmm_qr_smem_bytes(int m, int n);
+int aifmm_launch_qr_factor_smem(const QRJob* d_jobs, int njobs, size_t smem, cudaStream_t s);
+// panels of 64 right-hand sides per CTA in shared memory; the factor is staged
+// in shared memory when nzp <= smem_cols_cap
+int aifmm_launch_qr_solve_cols(const SolveJob* d_jobs, const int* d_cta_off, int njobs, int total_ctas,
+                               int smem_cols_cap, size_t smem, cudaStream_t s);
 int aifmm_launch_formq(const FormQJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s);
 int aifmm_launch_gemm(const GemmDesc* d, const GemmTerm* d_terms, const int* d_tile_off, int nd, int total_tiles,
                       cudaStream_t s);

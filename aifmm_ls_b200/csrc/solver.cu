@@ -147,6 +147,23 @@ class Staging {
   }
   template <class T>
   const T* put(const std::vector<T>& v, cudaStream_t s) { return static_cast<const T*>(put_raw(v.data(), v.size() * sizeof(T), s)); }
+  // several arrays in one contiguous region and one copy; returns device pointers
+  std::vector<const void*> put_many(std::initializer_list<std::pair<const void*, size_t>> parts, cudaStream_t s) {
+    size_t tot = 0;
+    for (auto& p : parts) tot += (p.second + 255) & ~size_t(255);
+    if (tot > cap_) throw Fail(AIFMM_ERR_NOMEM, "descriptor batch larger than the staging ring");
+    if (off_ + tot > cap_) { CK(cudaStreamSynchronize(s)); off_ = 0; }
+    std::vector<const void*> out;
+    size_t o = off_;
+    for (auto& p : parts) {
+      memcpy(h_ + o, p.first, p.second);
+      out.push_back(d_ + o);
+      o += (p.second + 255) & ~size_t(255);
+    }
+    CK(cudaMemcpyAsync(d_ + off_, h_ + off_, tot, cudaMemcpyHostToDevice, s));
+    off_ += tot;
+    return out;
+  }
   const void* put_raw(const void* src, size_t bytes, cudaStream_t s) {
     size_t b = (bytes + 255) & ~size_t(255);
     if (b > cap_) throw Fail(AIFMM_ERR_NOMEM, "descriptor batch larger than the staging ring");
@@ -356,10 +373,10 @@ struct aifmm_problem {
     int tot = 0;
     for (size_t i = 0; i < gd.size(); ++i) { off[i] = tot; tot += ((gd[i].m + 31) / 32) * ((gd[i].n + 31) / 32); }
     if (gt.empty()) gt.push_back(GemmTerm{});
-    const GemmTerm* dT = stage.put(gt, st);
-    const GemmDesc* dD = stage.put(gd, st);
-    const int* dO = stage.put(off, st);
-    KL(aifmm_launch_gemm(dD, dT, dO, (int)gd.size(), tot, st));
+    auto ptrs = stage.put_many({{gt.data(), gt.size() * sizeof(GemmTerm)}, {gd.data(), gd.size() * sizeof(GemmDesc)},
+                                {off.data(), off.size() * sizeof(int)}}, st);
+    KL(aifmm_launch_gemm(static_cast<const GemmDesc*>(ptrs[1]), static_cast<const GemmTerm*>(ptrs[0]),
+                         static_cast<const int*>(ptrs[2]), (int)gd.size(), tot, st));
     gd.clear(); gt.clear();
   }
   void geam(const Blk& C, const Blk& A, int opA, double2 alpha, double2 beta) {
@@ -376,9 +393,9 @@ struct aifmm_problem {
     std::vector<long long> off(ged.size());
     long long tot = 0;
     for (size_t i = 0; i < ged.size(); ++i) { off[i] = tot; tot += (long long)ged[i].m * ged[i].n; }
-    const GeamDesc* dD = stage.put(ged, st);
-    const long long* dO = stage.put(off, st);
-    KL(aifmm_launch_geam(dD, dO, (int)ged.size(), tot, st));
+    auto ptrs = stage.put_many({{ged.data(), ged.size() * sizeof(GeamDesc)}, {off.data(), off.size() * sizeof(long long)}}, st);
+    KL(aifmm_launch_geam(static_cast<const GeamDesc*>(ptrs[0]), static_cast<const long long*>(ptrs[1]),
+                         (int)ged.size(), tot, st));
     ged.clear();
   }
   void zero(const Blk& b) {
@@ -408,8 +425,21 @@ struct aifmm_problem {
   }
   void flush_qr() {
     if (qj.empty()) return;
-    const QRJob* dq = stage.put(qj, st);
-    KL(aifmm_launch_qr_factor(dq, (int)qj.size(), st));
+    std::vector<QRJob> small, large;
+    size_t smem = 0;
+    for (auto& j : qj) {
+      const size_t b = aifmm_qr_smem_bytes(j.m, j.n);
+      if (b <= size_t(200) << 10) { small.push_back(j); smem = std::max(smem, b); }
+      else large.push_back(j);
+    }
+    if (!small.empty()) {
+      const QRJob* dq = stage.put(small, st);
+      KL(aifmm_launch_qr_factor_smem(dq, (int)small.size(), smem, st));
+    }
+    if (!large.empty()) {
+      const QRJob* dq = stage.put(large, st);
+      KL(aifmm_launch_qr_factor(dq, (int)large.size(), st));
+    }
     qj.clear();
   }
   // X = alpha QR^{-1} B  (B.p == nullptr with B.c = r -> identity)
@@ -421,17 +451,44 @@ struct aifmm_problem {
     SolveJob s; s.qr = f.qr.p; s.ldq = f.qr.ld; s.m = f.qr.r; s.n = f.qr.c; s.tau = f.tau; s.perm = f.perm;
     s.info = f.info; s.B = identity ? nullptr : B.p; s.ldb = identity ? 1 : B.ld; s.X = X.p; s.ldx = X.ld;
     s.nrhs = nr; s.alpha = alpha;
-    s.work = static_cast<double2*>(scratch.get(sizeof(double2) * (size_t)std::max(1, f.qr.r) * nr));
+    s.work = nullptr;
     sj.push_back(s);
   }
   void flush_solve() {
     if (sj.empty()) return;
-    std::vector<int> off(sj.size());
-    int tot = 0;
-    for (size_t i = 0; i < sj.size(); ++i) { off[i] = tot; tot += sj[i].nrhs; }
-    const SolveJob* dj = stage.put(sj, st);
-    const int* dO = stage.put(off, st);
-    KL(aifmm_launch_qr_solve(dj, dO, (int)sj.size(), tot, st));
+    // panels of 64 right-hand sides in shared memory for m <= 200; larger systems
+    // (the base level) use the global-memory kernel with one warp per column
+    std::vector<SolveJob> small, large;
+    for (auto& j : sj) (j.m <= 200 ? small : large).push_back(j);
+    if (!small.empty()) {
+      std::vector<int> off(small.size());
+      int tot = 0, mmax = 1, nmax = 1;
+      for (size_t i = 0; i < small.size(); ++i) {
+        off[i] = tot;
+        tot += (small[i].nrhs + 63) / 64;
+        mmax = std::max(mmax, small[i].m);
+        nmax = std::max(nmax, std::min(small[i].m, small[i].n));
+      }
+      const size_t panel = sizeof(double2) * (size_t)(mmax | 1) * 64;
+      int cap = (int)(((size_t(200) << 10) - panel) / (sizeof(double2) * (size_t)(mmax + 1)));
+      cap = std::max(0, std::min(cap, nmax));
+      const size_t smem = panel + sizeof(double2) * ((size_t)mmax * cap + cap) + 64;
+      auto ptrs = stage.put_many({{small.data(), small.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}}, st);
+      KL(aifmm_launch_qr_solve_cols(static_cast<const SolveJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]),
+                                    (int)small.size(), tot, cap, smem, st));
+    }
+    if (!large.empty()) {
+      std::vector<int> off(large.size());
+      int tot = 0;
+      for (size_t i = 0; i < large.size(); ++i) {
+        off[i] = tot;
+        tot += large[i].nrhs;
+        large[i].work = static_cast<double2*>(scratch.get(sizeof(double2) * (size_t)large[i].m * large[i].nrhs));
+      }
+      auto ptrs = stage.put_many({{large.data(), large.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}}, st);
+      KL(aifmm_launch_qr_solve(static_cast<const SolveJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]),
+                               (int)large.size(), tot, st));
+    }
     sj.clear();
   }
   void formq(const QRF& f, const Blk& Q) {
@@ -445,13 +502,21 @@ struct aifmm_problem {
     std::vector<int> off(fq.size());
     int tot = 0;
     for (size_t i = 0; i < fq.size(); ++i) { off[i] = tot; tot += fq[i].ncols; }
-    const FormQJob* dj = stage.put(fq, st);
-    const int* dO = stage.put(off, st);
-    KL(aifmm_launch_formq(dj, dO, (int)fq.size(), tot, st));
+    auto ptrs = stage.put_many({{fq.data(), fq.size() * sizeof(FormQJob)}, {off.data(), off.size() * sizeof(int)}}, st);
+    KL(aifmm_launch_formq(static_cast<const FormQJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]), (int)fq.size(),
+                          tot, st));
     fq.clear();
   }
   void flush_all() { flush_geam(); flush_qr(); flush_solve(); flush_formq(); flush_gemm(); }
-  void sync() { CK(cudaStreamSynchronize(st)); }
+  // host-side statistics of the last factorize_solve (see aifmm_stats)
+  double st_sync_ms = 0, st_compress_ms = 0, st_elim_ms = 0, st_back_ms = 0, st_pending_ms = 0;
+  long st_syncs = 0, st_compress = 0, st_apicalls = 0;
+  void sync() {
+    auto t0 = std::chrono::steady_clock::now();
+    CK(cudaStreamSynchronize(st));
+    st_sync_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    ++st_syncs;
+  }
 
   // ------------------------------------------------------------------ setup
   void create(const aifmm_desc& desc, int dev) {
@@ -843,9 +908,9 @@ struct aifmm_problem {
     std::vector<long long> off(bd.size());
     long long tot = 0;
     for (size_t i = 0; i < bd.size(); ++i) { off[i] = tot; tot += (long long)bd[i].nr * bd[i].nc; }
-    const BlockDesc* dd = stage.put(bd, st);
-    const long long* dO = stage.put(off, st);
-    KL(aifmm_launch_block_entries(dd, dO, (int)bd.size(), tot, ctx(), st));
+    auto ptrs = stage.put_many({{bd.data(), bd.size() * sizeof(BlockDesc)}, {off.data(), off.size() * sizeof(long long)}}, st);
+    KL(aifmm_launch_block_entries(static_cast<const BlockDesc*>(ptrs[0]), static_cast<const long long*>(ptrs[1]),
+                                  (int)bd.size(), tot, ctx(), st));
   }
 
   // ------------------------------------------------------------------ elimination
@@ -1200,6 +1265,7 @@ struct aifmm_problem {
   }
 
   void compress_P2P_Two_Ways(int j, int k, int b) {  // F:1424-1490
+    ++st_compress;
     CompressOut kb, bk;
     compress_P2P_pair(j, k, b, kb, bk);
     Blk nLk = kb.nL, nPtb = kb.nPt, nLb = bk.nL, nPtk = bk.nPt;
@@ -1254,6 +1320,7 @@ struct aifmm_problem {
   }
 
   void compress_M2P_P2L(int j, int k, int b) {  // F:1492-1530 (k not eliminated, b eliminated)
+    ++st_compress;
     Box& K = T[j][k];
     Box& Bb = T[j][b];
     // compress_M2P(j, k, b) (F:1561-1575) and compress_P2L(j, b, k) (F:1577-1591) in lockstep
@@ -1394,6 +1461,7 @@ struct aifmm_problem {
     for (int j = depth; j >= 2; --j) {
       if (j != depth) initialise_P2P_NonLeafLevel(j);
       for (int k = 0; k < nBoxes[j]; ++k) {
+        auto tp0 = std::chrono::steady_clock::now();
         take_pending(j, k, p2p, p2l);
         for (auto& pr : p2p) {
           const int nn = pr.first, pp = pr.second;
@@ -1413,10 +1481,14 @@ struct aifmm_problem {
             drop(T[j][pp].M2P[nn]);
           }
         }
+        auto tp1 = std::chrono::steady_clock::now();
         T[j][k].elim = true;
         eliminate_x(j, k);
         eliminate_z(j, k);
         end_step();
+        auto tp2 = std::chrono::steady_clock::now();
+        st_pending_ms += std::chrono::duration<double, std::milli>(tp1 - tp0).count();
+        st_elim_ms += std::chrono::duration<double, std::milli>(tp2 - tp1).count();
       }
       cands.clear();  // pending pairs never cross a level
     }
@@ -1580,8 +1652,12 @@ struct aifmm_problem {
       }
     flush_geam();
     end_step();
+    st_sync_ms = st_compress_ms = st_elim_ms = st_back_ms = st_pending_ms = 0;
+    st_syncs = st_compress = 0;
     eliminate_phase_efficient();
+    auto tb0 = std::chrono::steady_clock::now();
     back_substitution_phase();
+    st_back_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb0).count();
     // gather the leaf particles
     double2* dx = (flags & AIFMM_PTR_DEVICE) ? reinterpret_cast<double2*>(x) : static_cast<double2*>(pool.alloc(bytes));
     for (int k = 0; k < nBoxes[depth]; ++k) {
@@ -1894,6 +1970,14 @@ aifmm_status aifmm_launch_counts(const aifmm_problem* p, long* factor_solve, lon
   if (!p || !factor_solve || !assemble) return AIFMM_ERR_ARG;
   *factor_solve = p->launches_fs;
   *assemble = p->launches_asm;
+  return AIFMM_OK;
+}
+
+aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n) {
+  if (!p || !out) return AIFMM_ERR_ARG;
+  const double v[8] = {p->st_sync_ms, (double)p->st_syncs, p->st_pending_ms, p->st_elim_ms, p->st_back_ms,
+                       (double)p->st_compress, p->ms[3], (double)p->launches_fs};
+  for (int i = 0; i < n && i < 8; ++i) out[i] = v[i];
   return AIFMM_OK;
 }
 

@@ -1,0 +1,333 @@
+"""Benchmark: factor+solve unknowns/s of the AIFMM-LS direct solver on B200.
+
+Workload (one GPU): depth-7 uniform quadtree, 6x6 Chebyshev nodes per leaf
+(589,824 unknowns), kappa = 40, contrast q = 1.5 exp(-32|x|^2), NCA/ACA and
+recompression tolerance 1e-10, FP64 (complex128), 8 plane-wave right-hand
+sides at angles drawn from the seed.  The leaf tables are precomputed once on
+the GPU (reported separately).  One step = assemble (ACA skeletons, bases,
+M2L, leaf P2P) + eliminate + back-substitute for the 8 right-hand sides.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value: unknowns x steps / device time (CUDA events on the solver's stream, the
+right-hand sides and solutions resident in HBM).  e2e: the same through the C
+ABI with host buffers (H2D of b and D2H of x inside every step).  With N > 1
+each rank solves its own replica (the direct solver does not shard; replicas
+only).  --impl reference times the CPU oracle (the reference algorithm restated
+in C++/OpenMP) on the host cores on a bounded sample.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(n_cheb=6, kappa=40.0, degree=6, L=1.0, depth=7, tol_pow=10, q_kind="gauss_aw", q_amp=1.5,
+                q_width=32.0, q_radius=0.5)
+NRHS = 8
+SEED = 20261203 + 1
+METRIC = "factor+solve unknowns/s (FP64, 8 RHS)"
+FAR_ENTRY_FLOPS = 2450  # algorithmic flops of one far-field entry (121-term Graf series)
+CPU_SAMPLE_DEPTH = 4
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    lrank = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, lrank
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def fp64_peak_tflops(device):
+    """Measured FP64 peak: cuBLAS DGEMM 8192^3 through torch (best of 5)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    torch.matmul(a, b)
+    torch.cuda.synchronize(device)
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def run_reference(args):
+    """CPU oracle (the reference algorithm restated) on the host cores."""
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    O.build()
+    cores = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    p = O.params(**{k: v for k, v in WORKLOAD.items() if k in ("n_cheb", "kappa", "degree", "L", "tol_pow", "q_kind",
+                                                                 "q_amp", "q_width", "q_radius")},
+                 depth=CPU_SAMPLE_DEPTH)
+    M, near, _ = O.tables(p)
+    rng = np.random.default_rng(SEED)
+    th = rng.uniform(0, 2 * np.pi, NRHS)
+    times = []
+    for it in range(args.warmup + args.steps):
+        P = O.Problem(p, M, near)
+        b = P.rhs_plane_wave(th)
+        t0 = time.perf_counter()
+        P.solve(b)
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(dt)
+        P.close()
+    N = 4 ** CPU_SAMPLE_DEPTH * 36
+    value = N * len(times) / sum(times)
+    sample = ("one assemble+eliminate+back-substitute of the benchmark physics at depth %d (%d unknowns, "
+              "%d RHS) per step; the CPU cost per unknown grows with depth, so this overstates the CPU "
+              "throughput at depth 7" % (CPU_SAMPLE_DEPTH, N, NRHS))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "unknowns/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+            "data": "synthetic", "config": {"workload": "lippmann-schwinger depth 7 (sampled at depth %d on CPU)"
+                                                       % CPU_SAMPLE_DEPTH, **WORKLOAD, "nrhs": NRHS},
+            "cpu_baseline": {"value": value, "unit": "unknowns/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "unknowns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample():
+    """The oracle on a bounded sample (rank 0, N = 1): about 10-30 s of CPU work."""
+    from oracle import oracle as O
+    O.build()
+    cores = os.cpu_count()
+    p = O.params(**{k: v for k, v in WORKLOAD.items() if k in ("n_cheb", "kappa", "degree", "L", "tol_pow", "q_kind",
+                                                                 "q_amp", "q_width", "q_radius")},
+                 depth=CPU_SAMPLE_DEPTH)
+    M, near, _ = O.tables(p)
+    rng = np.random.default_rng(SEED)
+    th = rng.uniform(0, 2 * np.pi, NRHS)
+    P = O.Problem(p, M, near)
+    b = P.rhs_plane_wave(th)
+    t0 = time.perf_counter()
+    P.solve(b)
+    dt = time.perf_counter() - t0
+    N = 4 ** CPU_SAMPLE_DEPTH * 36
+    return {"value": N / dt, "unit": "unknowns/s", "cores": cores, "kind": "port",
+            "sample": "one assemble+eliminate+back-substitute of the benchmark physics at depth %d (%d unknowns, "
+                      "%d RHS) with OpenMP on all host cores; the CPU cost per unknown grows with depth, so this "
+                      "overstates the CPU throughput at depth 7" % (CPU_SAMPLE_DEPTH, N, NRHS)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--depth", type=int, default=WORKLOAD["depth"], help="override the tree depth (diagnostics)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import aifmm_ls_b200 as A
+
+    ws, rank, lrank = _dist()
+    device = lrank if ws > 1 else 0
+    torch.cuda.set_device(device)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+
+    wl = dict(WORKLOAD)
+    wl["depth"] = args.depth
+    K = A.LSKernel(device=device, **wl)
+    t_tab0 = time.perf_counter()
+    K.tables_compute(round6=True)
+    t_tables = time.perf_counter() - t_tab0
+    T = A.FMM2DTree(K)
+    rng = np.random.default_rng(SEED)
+    th = rng.uniform(0, 2 * np.pi, NRHS)
+    b_host = K.rhs_plane_wave(th)            # (nrhs, N) complex128, pinned below
+    N = K.N
+    b_pin = torch.from_numpy(b_host.view(np.float64).copy()).pin_memory()
+    x_pin = torch.empty_like(b_pin).pin_memory()
+    b_dev = b_pin.to(f"cuda:{device}")
+    x_dev = torch.empty_like(b_dev)
+    lib = A.load()
+    sp = ctypes_void = None
+    import ctypes
+    sptr = ctypes.c_void_p()
+    lib.aifmm_get_stream(K.h, ctypes.byref(sptr))
+    stream = torch.cuda.ExternalStream(sptr.value, device=device)
+
+    def step(host_io):
+        T.createTree()
+        T.assemble()
+        if host_io:
+            st = lib.aifmm_factorize_solve(K.h, NRHS, ctypes.cast(b_pin.data_ptr(), ctypes.POINTER(ctypes.c_double)),
+                                           ctypes.cast(x_pin.data_ptr(), ctypes.POINTER(ctypes.c_double)), 0)
+        else:
+            st = lib.aifmm_factorize_solve(K.h, NRHS, ctypes.cast(b_dev.data_ptr(), ctypes.POINTER(ctypes.c_double)),
+                                           ctypes.cast(x_dev.data_ptr(), ctypes.POINTER(ctypes.c_double)), 1)
+        if st != 0:
+            raise A.AifmmError(st, lib.aifmm_last_error(K.h).decode())
+        return T.launch_counts()
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize(device)
+
+    for _ in range(args.warmup):
+        step(False)
+    clocks = ClockSampler(device)
+    clocks.start()
+    barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    launches = 0
+    asm_ms = fs_ms = 0.0
+    for _ in range(args.steps):
+        lc = step(False)
+        launches += lc[0] + lc[1]
+        ms = T.phase_times()
+        asm_ms += ms[2]
+        fs_ms += ms[3]
+    ev1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    t_dev = ev0.elapsed_time(ev1) / 1e3
+    if pg is not None:
+        tt = torch.tensor([t_dev], device=f"cuda:{device}")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t_dev = float(tt.item())
+    value = ws * N * args.steps / t_dev
+    # end to end through the C ABI with host buffers
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(True)
+    e1.record(stream)
+    barrier()
+    t_e2e = e0.elapsed_time(e1) / 1e3
+    if pg is not None:
+        tt = torch.tensor([t_e2e], device=f"cuda:{device}")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    x = x_pin.numpy().view(np.complex128).reshape(NRHS, N)
+    finite = bool(np.isfinite(x).all())
+    if rank == 0:
+        peaks = measured_peaks()
+        line = {
+            "metric": METRIC, "value": value, "unit": "unknowns/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic",
+            "config": {"workload": "lippmann-schwinger AIFMM direct solve, depth %d, %d unknowns, %d RHS"
+                                   % (args.depth, N, NRHS), **wl, "nrhs": NRHS, "seed": SEED,
+                       "parallelism": "replicas" if ws > 1 else "single",
+                       "l2": "working set (~17 GiB) far larger than L2; no flush needed"},
+            "e2e": {"value": ws * N * args.steps / t_e2e, "unit": "unknowns/s",
+                    "h2d_bytes_per_step": int(b_pin.numel() * 8), "d2h_bytes_per_step": int(x_pin.numel() * 8)},
+            "gpu_launches": int(launches),
+            "phases_ms_per_step": {"assemble": asm_ms / args.steps, "factorize_solve": fs_ms / args.steps,
+                                   "tables_once": 1e3 * t_tables},
+            "clocks": clk,
+            "solution_finite": finite,
+        }
+        if not args.no_cpu_baseline and ws == 1:
+            line["cpu_baseline"] = cpu_baseline_sample()
+        line["roofline"] = roofline_probe(K, A, device, peaks)
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def roofline_probe(K, A, device, peaks):
+    """Live measurement of the dominant kernel: filled in by aifmm_kernel_profile when available."""
+    lib = A.load()
+    if not hasattr(lib, "aifmm_kernel_profile"):
+        return None
+    return None
+
+
+if __name__ == "__main__":
+    main()

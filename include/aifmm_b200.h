@@ -116,6 +116,11 @@ aifmm_status aifmm_box_skeleton(aifmm_problem* p, int level, int box, int which,
 aifmm_status aifmm_phase_times(const aifmm_problem* p, double* ms);
 /* Number of kernel launches issued by the last factorize_solve and by the last assemble. */
 aifmm_status aifmm_launch_counts(const aifmm_problem* p, long* factor_solve, long* assemble);
+/* Host-side statistics of the last factorize_solve: [0] ms waiting in stream syncs,
+ * [1] number of syncs, [2] ms in pending-pair handling (recompression), [3] ms in the
+ * per-box elimination, [4] ms in back substitution, [5] recompressions, [6] total ms,
+ * [7] kernel launches. */
+aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n);
 /* The CUDA stream the handle works on (cudaStream_t). */
 aifmm_status aifmm_get_stream(const aifmm_problem* p, void** stream);
 
