@@ -38,6 +38,8 @@ def build(verbose=False, jobs=None):
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
     headers.append(os.path.join(ROOT, "include", "aifmm_b200.h"))
+    headers.append(os.path.join(ROOT, "include", "aifmm_fmm2dtree.hpp"))
+    headers.append(os.path.join(HERE, "cli", "testFMM2D_find_error.cpp"))
     newest_dep = max(os.path.getmtime(p) for p in srcs + headers)
     if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest_dep:
         return LIB
@@ -62,6 +64,11 @@ def build(verbose=False, jobs=None):
     cmd = [nvcc()] + ARCH + ["-shared", "-ccbin", _host_cxx(), "-o", tmp] + objs + ["-lcudart"]
     subprocess.check_call(cmd)
     os.replace(tmp, LIB)
+    # the reference driver's command line, on the C++ surface of include/aifmm_fmm2dtree.hpp
+    cli = os.path.join(HERE, "cli", "testFMM2D_find_error.cpp")
+    subprocess.check_call([_host_cxx(), "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), cli,
+                           "-L", LIBDIR, "-laifmm_b200", "-Wl,-rpath,$ORIGIN", "-o",
+                           os.path.join(LIBDIR, "testFMM2D_find_error")])
     return LIB
 
 
