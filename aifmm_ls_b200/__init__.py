@@ -55,6 +55,7 @@ SIGNATURES = {
     "aifmm_tables_compute": ([_v, ctypes.c_int], ctypes.c_int),
     "aifmm_tables_set": ([_v, _d, _d], ctypes.c_int),
     "aifmm_tables_get": ([_v, _d, _d], ctypes.c_int),
+    "aifmm_tables_compute_noalloc": ([_v, _v, _v], ctypes.c_int),
     "aifmm_num_points": ([_v, _i], ctypes.c_int),
     "aifmm_grid_points": ([_v, _d], ctypes.c_int),
     "aifmm_rhs_plane_wave": ([_v, ctypes.c_int, _d, _d, ctypes.c_int], ctypes.c_int),

@@ -1734,6 +1734,83 @@ struct aifmm_problem {
 };
 
 // ============================================================================
+// Leaf tables without allocation (aifmm_tables_compute_noalloc)
+//
+// Some callers cannot let a library call cudaMalloc: applications that reserve
+// the GPU's memory up front and hand out every byte through their own
+// allocator, and latency-sensitive loops for which the device synchronisation
+// that cudaMalloc / cudaFree may imply is not acceptable.  For them the table
+// quadrature has a variant whose scratch (far-field moments, near-field
+// integrals, the pseudo-inverse, a status word) lives in one file-scope device
+// array of kTablesScratchBytes.  Every GPU that loads this library holds that
+// array until the process exits.
+// ============================================================================
+namespace {
+constexpr size_t kTablesScratchBytes = size_t(1) << 20;  // 1 MiB
+__device__ __align__(256) unsigned char g_tables_scratch[kTablesScratchBytes];
+constexpr int kMaxDevices = 64;
+void* g_scratch_addr[kMaxDevices] = {nullptr};
+}  // namespace
+
+extern "C" aifmm_status aifmm_tables_compute_noalloc(aifmm_problem* p, double* M_dev, double* near_dev) {
+  if (!p || !M_dev || !near_dev) return AIFMM_ERR_ARG;
+  if (cudaSetDevice(p->device) != cudaSuccess) return AIFMM_ERR_CUDA;
+  if (p->device < 0 || p->device >= kMaxDevices) return AIFMM_ERR_ARG;
+  // the symbol's device address, looked up once per device with that device current
+  void*& base = g_scratch_addr[p->device];
+  if (!base) {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_tables_scratch) != cudaSuccess || !ptr) return AIFMM_ERR_CUDA;
+    base = ptr;
+  }
+  const int rank = p->rank, nb = p->nb;
+  // scratch layout: C (121 x nb) | V (9 rank x nb) | Q^+ (nb x rank doubles) | status
+  const size_t offC = 0;
+  const size_t offV = (offC + sizeof(double2) * 121 * (size_t)nb + 255) & ~size_t(255);
+  const size_t offQ = (offV + sizeof(double2) * 9 * (size_t)rank * nb + 255) & ~size_t(255);
+  const size_t offS = (offQ + sizeof(double) * (size_t)nb * rank + 255) & ~size_t(255);
+  if (offS + sizeof(int) > kTablesScratchBytes) return AIFMM_ERR_ARG;  // problem larger than the fixed scratch
+  char* sc = static_cast<char*>(base);
+  double2* Cw = reinterpret_cast<double2*>(sc + offC);
+  double2* Vw = reinterpret_cast<double2*>(sc + offV);
+  double* qp = reinterpret_cast<double*>(sc + offQ);
+  int* status = reinterpret_cast<int*>(sc + offS);
+  // small inputs from fixed-size host arrays through the handle's preallocated pinned ring
+  double glx[10], glw[10];
+  gauss_legendre10(glx, glw);
+  int2 basis[64];
+  int t = 0;
+  for (int dd = 0; dd < p->d.degree; ++dd)
+    for (int a = 0; a < dd + 1; ++a) basis[t++] = make_int2(a, dd - a);  // LS/FarFieldInteraction.hpp:46-54
+  double cheb[16];
+  const double PI = 3.1415926535897932384;
+  for (int k = 0; k < p->d.n_cheb; ++k) cheb[k] = -std::cos((k + 0.5) / p->d.n_cheb * PI);
+  double r = p->d.L;
+  for (int j = 0; j < p->depth; ++j) r = r / 2.0;
+  const double* dx;
+  const double* dw;
+  const int2* db;
+  const double* dc;
+  try {
+    dx = static_cast<const double*>(p->stage.put_raw(glx, sizeof glx, p->st));
+    dw = static_cast<const double*>(p->stage.put_raw(glw, sizeof glw, p->st));
+    db = static_cast<const int2*>(p->stage.put_raw(basis, sizeof(int2) * nb, p->st));
+    dc = static_cast<const double*>(p->stage.put_raw(cheb, sizeof(double) * p->d.n_cheb, p->st));
+  } catch (...) {
+    return AIFMM_ERR_CUDA;
+  }
+  // the array keeps the previous call's contents: the status word must start at zero
+  if (cudaMemsetAsync(status, 0, sizeof(int), p->st) != cudaSuccess) return AIFMM_ERR_CUDA;
+  if (aifmm_launch_tables(p->d.n_cheb, p->d.degree, p->d.kappa, r, dx, dw, db, dc, Cw, Vw, status, qp,
+                          reinterpret_cast<double2*>(M_dev), reinterpret_cast<double2*>(near_dev), p->st) != 0)
+    return AIFMM_ERR_CUDA;
+  int h_status = 0;
+  if (cudaMemcpyAsync(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost, p->st) != cudaSuccess) return AIFMM_ERR_CUDA;
+  if (cudaStreamSynchronize(p->st) != cudaSuccess) return AIFMM_ERR_CUDA;
+  return h_status ? AIFMM_ERR_NUMERIC : AIFMM_OK;
+}
+
+// ============================================================================
 // C ABI
 // ============================================================================
 namespace {

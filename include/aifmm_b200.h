@@ -74,6 +74,24 @@ const char* aifmm_status_string(aifmm_status s);
  * (rank x rank each), by adaptive Gauss-Legendre quadrature on the GPU.  round6 != 0
  * applies the reference's text round trip (6 significant digits) to both. */
 aifmm_status aifmm_tables_compute(aifmm_problem* p, int round6);
+/* No counterpart in the reference.  The tables of aifmm_tables_compute(p, 0) (no
+ * 6-digit round trip) written to caller-provided device buffers M_dev (121 x rank
+ * complex) and near_dev (9 x rank x rank complex), without any device or host
+ * allocation.  It is meant for callers that cannot let a library call cudaMalloc:
+ * applications that reserve all device memory up front and hand it out through
+ * their own allocator, and latency-sensitive loops that cannot accept the device
+ * synchronisation cudaMalloc / cudaFree may cause.
+ *  - Scratch is one fixed 1 MiB device array inside the library, held by every GPU
+ *    that loads the library until the process exits; problems whose scratch
+ *    (C 121 x NB, V 9 rank x NB, Q^+ NB x rank, 256-byte aligned) exceeds it are
+ *    rejected with AIFMM_ERR_ARG (e.g. 16 x 16 nodes with degree >= 10).
+ *  - The first call on a device looks up the array's device address; make that
+ *    first call before any stream capture.
+ *  - Runs on the handle's stream and returns when the tables are written.
+ *  - All calls share the array: calls that overlap on the GPU (other handles,
+ *    other host threads) race and must be serialised by the caller.
+ *  - aifmm_last_error() is not updated by this call; the status is the error. */
+aifmm_status aifmm_tables_compute_noalloc(aifmm_problem* p, double* M_dev, double* near_dev);
 /* Supply / read the tables (host memory, interleaved complex, column-major:
  * M is 121 x rank, near is 9 consecutive rank x rank tables). */
 aifmm_status aifmm_tables_set(aifmm_problem* p, const double* M, const double* near_tables);
