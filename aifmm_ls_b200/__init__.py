@@ -71,6 +71,8 @@ SIGNATURES = {
     "aifmm_launch_counts": ([_v, _P(ctypes.c_long), _P(ctypes.c_long)], ctypes.c_int),
     "aifmm_get_stream": ([_v, _P(_v)], ctypes.c_int),
     "aifmm_stats": ([_v, _d, ctypes.c_int], ctypes.c_int),
+    "aifmm_kernel_profile": ([_v, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "aifmm_kernel_profile_read": ([_v, ctypes.c_int, _P(ctypes.c_long), _d, _d], ctypes.c_int),
 }
 
 
@@ -275,6 +277,16 @@ class FMM2DTree:
         self._ck(load().aifmm_stats(self.K.h, _dp(v), 8))
         keys = ["sync_ms", "syncs", "pending_ms", "elim_ms", "back_ms", "compressions", "total_ms", "launches"]
         return dict(zip(keys, v.tolist()))
+
+    def kernel_profile(self, kind, enable=True):
+        self._ck(load().aifmm_kernel_profile(self.K.h, kind, 1 if enable else 0))
+
+    def kernel_profile_read(self, kind):
+        n = ctypes.c_long()
+        ms = ctypes.c_double()
+        fl = ctypes.c_double()
+        self._ck(load().aifmm_kernel_profile_read(self.K.h, kind, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(fl)))
+        return n.value, ms.value, fl.value
 
     def launch_counts(self):
         a = ctypes.c_long()

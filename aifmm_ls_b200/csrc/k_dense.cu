@@ -202,7 +202,8 @@ __global__ void __launch_bounds__(kT) qr_factor_smem_kernel(const QRJob* __restr
   double2* A = smem;  // m x n
   double* nu = reinterpret_cast<double*>(A + (size_t)ld * n);
   double* nd = nu + n;
-  int* perm = reinterpret_cast<int*>(nd + n);
+  double2* wcol = reinterpret_cast<double2*>(nd + n);  // v^H a_j of the current step
+  int* perm = reinterpret_cast<int*>(wcol + n);
   for (int e = tid; e < m * n; e += kT) {
     const int i = e % m, j = e / m;
     A[i + (size_t)j * ld] = J.a[i + (size_t)j * J.lda];
@@ -269,7 +270,8 @@ __global__ void __launch_bounds__(kT) qr_factor_smem_kernel(const QRJob* __restr
         if (c0.x >= 0.0) beta = -beta;
         const double2 den = make_double2(c0.x - beta, c0.y);
         t = cconj(cdiv(make_double2(beta - c0.x, -c0.y), make_double2(beta, 0.0)));
-        for (int i = k + 1 + lane; i < m; i += 32) A[i + (size_t)k * ld] = cdiv(A[i + (size_t)k * ld], den);
+        const double2 rden = cdiv(make_double2(1.0, 0.0), den);
+        for (int i = k + 1 + lane; i < m; i += 32) A[i + (size_t)k * ld] = cmul(A[i + (size_t)k * ld], rden);
       }
       __syncwarp();
       if (lane == 0) { A[k + (size_t)k * ld] = make_double2(beta, 0.0); s_tau = t; s_beta = beta; J.tau[k] = t; }
@@ -277,17 +279,47 @@ __global__ void __launch_bounds__(kT) qr_factor_smem_kernel(const QRJob* __restr
     __syncthreads();
     const double2 t = s_tau;
     maxpivot = fmax(maxpivot, fabs(s_beta));
-    // apply G = I - t v v^H to the columns this thread owns, then downdate their norms
+    // apply G = I - t v v^H to columns k+1..n-1: dot products with 4 threads per
+    // column, the rank-1 update over all threads, norm downdates per column
     const double2* v = A + (size_t)k * ld;
+    const int ncol = n - k - 1;
+    for (int base = 0; base < ncol; base += kT / 4) {
+      const int cj = base + (tid >> 2), part = tid & 3;
+      double2 sdot = make_double2(0.0, 0.0);
+      if (cj < ncol) {
+        const double2* col = A + (size_t)(k + 1 + cj) * ld;
+        for (int i = k + 1 + part; i < m; i += 4) sdot = cfmac(v[i], col[i], sdot);
+      }
+      sdot.x += __shfl_xor_sync(0xffffffffu, sdot.x, 1); sdot.y += __shfl_xor_sync(0xffffffffu, sdot.y, 1);
+      sdot.x += __shfl_xor_sync(0xffffffffu, sdot.x, 2); sdot.y += __shfl_xor_sync(0xffffffffu, sdot.y, 2);
+      if (cj < ncol && part == 0) wcol[cj] = cadd(A[k + (size_t)(k + 1 + cj) * ld], sdot);
+    }
+    __syncthreads();
+    {
+      const int rows = m - k;
+      const long tot = (long)rows * ncol;
+      for (long e0 = tid; e0 < tot; e0 += 4L * kT) {
+        double2 a[4], f[4];
+        int ii[4], jj[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const long e = e0 + (long)u * kT;
+          ii[u] = -1;
+          if (e < tot) {
+            ii[u] = k + (int)(e % rows);
+            jj[u] = (int)(e / rows);
+            a[u] = A[ii[u] + (size_t)(k + 1 + jj[u]) * ld];
+            f[u] = ii[u] == k ? t : cmul(t, v[ii[u]]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (ii[u] >= 0) A[ii[u] + (size_t)(k + 1 + jj[u]) * ld] = csub(a[u], cmul(f[u], wcol[jj[u]]));
+      }
+    }
+    __syncthreads();
     for (int j = k + 1 + tid; j < n; j += kT) {
       double2* col = A + (size_t)j * ld;
-      double2 s0 = make_double2(0.0, 0.0), s1 = make_double2(0.0, 0.0);
-      int i = k + 1;
-      for (; i + 1 < m; i += 2) { s0 = cfmac(v[i], col[i], s0); s1 = cfmac(v[i + 1], col[i + 1], s1); }
-      if (i < m) s0 = cfmac(v[i], col[i], s0);
-      const double2 wv = cadd(col[k], cadd(s0, s1));
-      for (int r = k + 1; r < m; ++r) col[r] = csub(col[r], cmul(cmul(t, v[r]), wv));
-      col[k] = csub(col[k], cmul(t, wv));
       const double upd = nu[j];
       if (upd != 0.0) {
         double tmp = cabsd(col[k]) / upd;
@@ -320,6 +352,92 @@ __global__ void __launch_bounds__(kT) qr_factor_smem_kernel(const QRJob* __restr
     J.info[0] = nzp;
     J.info[1] = rk;
     if (J.maxpiv) J.maxpiv[0] = maxpivot;
+  }
+}
+
+// ---------------------------------------------------------------- QR solve (warp per column, registers)
+// One warp per right-hand side; lane l holds rows l, l+32, ... of its column in
+// registers (RPL rows per lane, m <= 32*RPL).  The first nzp columns of the
+// factor and tau are staged once per CTA in shared memory.  Only warp shuffles
+// synchronise: Q^H b reflector by reflector, then column-oriented back
+// substitution with R, then the column permutation.
+template <int RPL>
+__global__ void __launch_bounds__(kT) qr_solve_warp_kernel(const SolveJob* __restrict__ jobs,
+                                                           const int* __restrict__ cta_off, int njobs) {
+  extern __shared__ double2 fsm[];
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cta_off[mid] <= (int)blockIdx.x) lo = mid; else hi = mid - 1; }
+  const SolveJob J = jobs[lo];
+  const int m = J.m, n = J.n, nzp = J.info[0];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int c = (blockIdx.x - cta_off[lo]) * kW + w;
+  const int ldf = m | 1;
+  double2* F = fsm;                      // m x nzp, ld = m|1
+  double2* tau = fsm + (size_t)ldf * nzp;
+  for (int e = threadIdx.x; e < m * nzp; e += kT) {
+    const int i = e % m, j = e / m;
+    F[i + (size_t)j * ldf] = J.qr[i + (size_t)j * J.ldq];
+  }
+  for (int k = threadIdx.x; k < nzp; k += kT) tau[k] = J.tau[k];
+  __syncthreads();
+  if (c >= J.nrhs) return;
+  double2* x = J.X + (size_t)c * J.ldx;
+  if (nzp == 0) {
+    for (int i = lane; i < n; i += 32) x[i] = make_double2(0.0, 0.0);
+    return;
+  }
+  double2 b[RPL];
+#pragma unroll
+  for (int r = 0; r < RPL; ++r) {
+    const int i = lane + 32 * r;
+    b[r] = i < m ? (J.B ? J.B[i + (size_t)c * J.ldb] : make_double2(i == c ? 1.0 : 0.0, 0.0)) : make_double2(0.0, 0.0);
+  }
+  for (int k = 0; k < nzp; ++k) {
+    const double2* v = F + (size_t)k * ldf;
+    double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int i = lane + 32 * r;
+      if (i > k && i < m) s = cfmac(v[i], b[r], s);
+    }
+    s = warp_sum2(s);
+    const int ok = k & 31, rk = k >> 5;
+    double2 bk = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) if (r == rk) bk = b[r];
+    bk.x = __shfl_sync(0xffffffffu, bk.x, ok);
+    bk.y = __shfl_sync(0xffffffffu, bk.y, ok);
+    const double2 t = tau[k];
+    const double2 wv = cadd(bk, s);
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int i = lane + 32 * r;
+      if (i > k && i < m) b[r] = csub(b[r], cmul(cmul(t, v[i]), wv));
+      else if (i == k) b[r] = csub(b[r], cmul(t, wv));
+    }
+  }
+  for (int i = nzp - 1; i >= 0; --i) {
+    const int oi = i & 31, ri = i >> 5;
+    double2 bi = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) if (r == ri) bi = b[r];
+    bi.x = __shfl_sync(0xffffffffu, bi.x, oi);
+    bi.y = __shfl_sync(0xffffffffu, bi.y, oi);
+    const double2 xi = cdiv(bi, F[i + (size_t)i * ldf]);
+    const double2* Rc = F + (size_t)i * ldf;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+      const int l = lane + 32 * r;
+      if (l < i) b[r] = csub(b[r], cmul(Rc[l], xi));
+      else if (l == i) b[r] = xi;
+    }
+  }
+  for (int i = lane; i < n; i += 32) x[i] = make_double2(0.0, 0.0);
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < RPL; ++r) {
+    const int i = lane + 32 * r;
+    if (i < nzp) x[J.perm[i]] = cmul(J.alpha, b[r]);
   }
 }
 
@@ -387,12 +505,26 @@ __global__ void __launch_bounds__(kT) qr_solve_cols_kernel(const SolveJob* __res
       s.x += __shfl_xor_sync(0xffffffffu, s.x, 2); s.y += __shfl_xor_sync(0xffffffffu, s.y, 2);
     }
     __syncthreads();
-    for (int e = tid; e < (m - k) * nc; e += kT) {
-      const int i = k + e % (m - k), cc = e / (m - k);
-      const double2 tw = wdot[cc];
-      double2* bb = B + i + (size_t)cc * ldb;
-      if (i == k) *bb = csub(*bb, tw);
-      else *bb = csub(*bb, cmul(v[i], tw));
+    {
+      const int rows = m - k, tot = rows * nc;
+      for (int e0 = tid; e0 < tot; e0 += 4 * kT) {
+        double2 bv[4], f[4];
+        int off[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int e = e0 + u * kT;
+          off[u] = -1;
+          if (e < tot) {
+            const int i = k + e % rows, cc = e / rows;
+            off[u] = i + cc * ldb;
+            bv[u] = B[off[u]];
+            f[u] = i == k ? wdot[cc] : cmul(v[i], wdot[cc]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (off[u] >= 0) B[off[u]] = csub(bv[u], f[u]);
+      }
     }
     __syncthreads();
   }
@@ -400,9 +532,26 @@ __global__ void __launch_bounds__(kT) qr_solve_cols_kernel(const SolveJob* __res
     const double2 rii = Q[i + (size_t)i * ldq];
     for (int cc = tid; cc < nc; cc += kT) B[i + (size_t)cc * ldb] = cdiv(B[i + (size_t)cc * ldb], rii);
     __syncthreads();
-    for (int e = tid; e < i * nc; e += kT) {
-      const int l = e % i, cc = e / i;
-      B[l + (size_t)cc * ldb] = csub(B[l + (size_t)cc * ldb], cmul(Q[l + (size_t)i * ldq], B[i + (size_t)cc * ldb]));
+    {
+      const int tot = i * nc;
+      for (int e0 = tid; e0 < tot; e0 += 4 * kT) {
+        double2 bv[4], f[4];
+        int off[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int e = e0 + u * kT;
+          off[u] = -1;
+          if (e < tot) {
+            const int l = e % i, cc = e / i;
+            off[u] = l + cc * ldb;
+            bv[u] = B[off[u]];
+            f[u] = cmul(Q[l + (size_t)i * ldq], B[i + cc * ldb]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (off[u] >= 0) B[off[u]] = csub(bv[u], f[u]);
+      }
     }
     __syncthreads();
   }
@@ -660,8 +809,32 @@ int aifmm_launch_qr_factor(const QRJob* d_jobs, int njobs, cudaStream_t s) {
   qr_factor_kernel<<<njobs, kT, 0, s>>>(d_jobs);
   return (int)cudaGetLastError();
 }
+int aifmm_launch_qr_solve_warp(const SolveJob* d_jobs, const int* d_cta_off, int njobs, int total_ctas, int mmax,
+                               int nzpmax, cudaStream_t s) {
+  if (njobs <= 0 || total_ctas <= 0) return 0;
+  const size_t smem = sizeof(double2) * ((size_t)(mmax | 1) * nzpmax + nzpmax) + 64;
+  const int rpl = (mmax + 31) / 32;
+  static bool attr[8] = {false};
+  switch (rpl) {
+#define AIFMM_SOLVE_CASE(R)                                                                            \
+    case R:                                                                                            \
+      if (!attr[R]) {                                                                                  \
+        cudaFuncSetAttribute(qr_solve_warp_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024); \
+        attr[R] = true;                                                                                \
+      }                                                                                                \
+      qr_solve_warp_kernel<R><<<total_ctas, kT, smem, s>>>(d_jobs, d_cta_off, njobs);                  \
+      break;
+    AIFMM_SOLVE_CASE(1) AIFMM_SOLVE_CASE(2) AIFMM_SOLVE_CASE(3) AIFMM_SOLVE_CASE(4)
+    AIFMM_SOLVE_CASE(5) AIFMM_SOLVE_CASE(6) AIFMM_SOLVE_CASE(7)
+#undef AIFMM_SOLVE_CASE
+    default: return (int)cudaErrorInvalidValue;
+  }
+  return (int)cudaGetLastError();
+}
+
 size_t aifmm_qr_smem_bytes(int m, int n) {
-  return sizeof(double2) * (size_t)(m | 1) * n + sizeof(double) * 2 * (size_t)n + sizeof(int) * (size_t)n + 64;
+  return sizeof(double2) * (size_t)(m | 1) * n + sizeof(double) * 2 * (size_t)n + sizeof(double2) * (size_t)n +
+         sizeof(int) * (size_t)n + 64;
 }
 int aifmm_launch_qr_factor_smem(const QRJob* d_jobs, int njobs, size_t smem, cudaStream_t s) {
   if (njobs <= 0) return 0;

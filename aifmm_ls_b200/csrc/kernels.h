@@ -106,6 +106,10 @@ int aifmm_launch_aca(const AcaJob* d_jobs, int njobs, double tol, const EntryCtx
 int aifmm_launch_qr_factor(const QRJob* d_jobs, int njobs, cudaStream_t s);
 int aifmm_launch_qr_solve(const SolveJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s);
 size_t aifmm_qr_smem_bytes(int m, int n);
+// one warp per right-hand side (8 per CTA), the column in registers; m <= 224 and
+// the factor's first nzp columns must fit in shared memory
+int aifmm_launch_qr_solve_warp(const SolveJob* d_jobs, const int* d_cta_off, int njobs, int total_ctas, int mmax,
+                               int nzpmax, cudaStream_t s);
 int aifmm_launch_qr_factor_smem(const QRJob* d_jobs, int njobs, size_t smem, cudaStream_t s);
 // panels of 64 right-hand sides per CTA in shared memory; the factor is staged
 // in shared memory when nzp <= smem_cols_cap

@@ -372,11 +372,17 @@ struct aifmm_problem {
     std::vector<int> off(gd.size());
     int tot = 0;
     for (size_t i = 0; i < gd.size(); ++i) { off[i] = tot; tot += ((gd[i].m + 31) / 32) * ((gd[i].n + 31) / 32); }
+    double fl = 0;
+    for (auto& g : gd)
+      for (int t = 0; t < g.nterms; ++t) fl += 8.0 * g.m * g.n * gt[g.term0 + t].k;
     if (gt.empty()) gt.push_back(GemmTerm{});
     auto ptrs = stage.put_many({{gt.data(), gt.size() * sizeof(GemmTerm)}, {gd.data(), gd.size() * sizeof(GemmDesc)},
                                 {off.data(), off.size() * sizeof(int)}}, st);
+    cudaEvent_t a;
+    const bool pr = prof_begin(2, a);
     KL(aifmm_launch_gemm(static_cast<const GemmDesc*>(ptrs[1]), static_cast<const GemmTerm*>(ptrs[0]),
                          static_cast<const int*>(ptrs[2]), (int)gd.size(), tot, st));
+    if (pr) prof_end(2, a, fl);
     gd.clear(); gt.clear();
   }
   void geam(const Blk& C, const Blk& A, int opA, double2 alpha, double2 beta) {
@@ -427,18 +433,25 @@ struct aifmm_problem {
     if (qj.empty()) return;
     std::vector<QRJob> small, large;
     size_t smem = 0;
+    double fl_small = 0, fl_large = 0;
     for (auto& j : qj) {
       const size_t b = aifmm_qr_smem_bytes(j.m, j.n);
-      if (b <= size_t(200) << 10) { small.push_back(j); smem = std::max(smem, b); }
-      else large.push_back(j);
+      if (b <= size_t(200) << 10) { small.push_back(j); smem = std::max(smem, b); fl_small += qr_flops(j.m, j.n); }
+      else { large.push_back(j); fl_large += qr_flops(j.m, j.n); }
     }
     if (!small.empty()) {
       const QRJob* dq = stage.put(small, st);
+      cudaEvent_t a;
+      const bool pr = prof_begin(0, a);
       KL(aifmm_launch_qr_factor_smem(dq, (int)small.size(), smem, st));
+      if (pr) prof_end(0, a, fl_small);
     }
     if (!large.empty()) {
       const QRJob* dq = stage.put(large, st);
+      cudaEvent_t a;
+      const bool pr = prof_begin(0, a);
       KL(aifmm_launch_qr_factor(dq, (int)large.size(), st));
+      if (pr) prof_end(0, a, fl_large);
     }
     qj.clear();
   }
@@ -456,26 +469,38 @@ struct aifmm_problem {
   }
   void flush_solve() {
     if (sj.empty()) return;
-    // panels of 64 right-hand sides in shared memory for m <= 200; larger systems
-    // (the base level) use the global-memory kernel with one warp per column
+    // m <= 224 whose factor fits in shared memory: one warp per column with the
+    // column in registers; larger systems (the base level): the global-memory kernel
     std::vector<SolveJob> small, large;
-    for (auto& j : sj) (j.m <= 200 ? small : large).push_back(j);
+    int mmax = 1, nmax = 1;
+    for (auto& j : sj) {
+      const int s_ = std::min(j.m, j.n);
+      const size_t need = sizeof(double2) * ((size_t)(j.m | 1) * s_ + s_);
+      if (j.m <= 224 && need <= (size_t(200) << 10)) {
+        small.push_back(j);
+        mmax = std::max(mmax, j.m);
+        nmax = std::max(nmax, s_);
+      } else {
+        large.push_back(j);
+      }
+    }
+    if (sizeof(double2) * ((size_t)(mmax | 1) * nmax + nmax) > (size_t(200) << 10)) {
+      // the batch's largest m and rank do not fit together: split by size
+      for (auto& j : small) large.push_back(j);
+      small.clear();
+    }
     if (!small.empty()) {
       std::vector<int> off(small.size());
-      int tot = 0, mmax = 1, nmax = 1;
-      for (size_t i = 0; i < small.size(); ++i) {
-        off[i] = tot;
-        tot += (small[i].nrhs + 63) / 64;
-        mmax = std::max(mmax, small[i].m);
-        nmax = std::max(nmax, std::min(small[i].m, small[i].n));
-      }
-      const size_t panel = sizeof(double2) * (size_t)(mmax | 1) * 64;
-      int cap = (int)(((size_t(200) << 10) - panel) / (sizeof(double2) * (size_t)(mmax + 1)));
-      cap = std::max(0, std::min(cap, nmax));
-      const size_t smem = panel + sizeof(double2) * ((size_t)mmax * cap + cap) + 64;
+      int tot = 0;
+      for (size_t i = 0; i < small.size(); ++i) { off[i] = tot; tot += (small[i].nrhs + 7) / 8; }
       auto ptrs = stage.put_many({{small.data(), small.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}}, st);
-      KL(aifmm_launch_qr_solve_cols(static_cast<const SolveJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]),
-                                    (int)small.size(), tot, cap, smem, st));
+      double fl = 0;
+      for (auto& j : small) { const double mz = std::min(j.m, j.n); fl += (16.0 * j.m * mz - 4.0 * mz * mz) * j.nrhs; }
+      cudaEvent_t a;
+      const bool pr = prof_begin(1, a);
+      KL(aifmm_launch_qr_solve_warp(static_cast<const SolveJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]),
+                                    (int)small.size(), tot, mmax, nmax, st));
+      if (pr) prof_end(1, a, fl);
     }
     if (!large.empty()) {
       std::vector<int> off(large.size());
@@ -486,8 +511,13 @@ struct aifmm_problem {
         large[i].work = static_cast<double2*>(scratch.get(sizeof(double2) * (size_t)large[i].m * large[i].nrhs));
       }
       auto ptrs = stage.put_many({{large.data(), large.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}}, st);
+      double fl = 0;
+      for (auto& j : large) { const double mz = std::min(j.m, j.n); fl += (16.0 * j.m * mz - 4.0 * mz * mz) * j.nrhs; }
+      cudaEvent_t a;
+      const bool pr = prof_begin(1, a);
       KL(aifmm_launch_qr_solve(static_cast<const SolveJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]),
                                (int)large.size(), tot, st));
+      if (pr) prof_end(1, a, fl);
     }
     sj.clear();
   }
@@ -508,6 +538,53 @@ struct aifmm_problem {
     fq.clear();
   }
   void flush_all() { flush_geam(); flush_qr(); flush_solve(); flush_formq(); flush_gemm(); }
+  // Optional CUDA-event timing of selected kernel kinds (aifmm_kernel_profile).
+  // kinds: 0 QR factorisation, 1 QR solve, 2 GEMM, 3 ACA, 4 entry blocks, 5 GEAM
+  static constexpr int kKinds = 6;
+  bool prof_on[kKinds] = {false, false, false, false, false, false};
+  struct ProfRec { cudaEvent_t a, b; double flops; };
+  std::vector<ProfRec> prof_pending[kKinds];
+  std::vector<cudaEvent_t> prof_free;
+  long prof_launches[kKinds] = {0, 0, 0, 0, 0, 0};
+  double prof_ms[kKinds] = {0, 0, 0, 0, 0, 0}, prof_flops[kKinds] = {0, 0, 0, 0, 0, 0};
+  cudaEvent_t prof_event() {
+    if (!prof_free.empty()) { cudaEvent_t e = prof_free.back(); prof_free.pop_back(); return e; }
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    return e;
+  }
+  bool prof_begin(int kind, cudaEvent_t& a) {
+    if (!prof_on[kind]) return false;
+    a = prof_event();
+    CK(cudaEventRecord(a, st));
+    return true;
+  }
+  void prof_end(int kind, cudaEvent_t a, double flops) {
+    cudaEvent_t b = prof_event();
+    CK(cudaEventRecord(b, st));
+    prof_pending[kind].push_back({a, b, flops});
+    if (prof_pending[kind].size() > 4096) prof_collect();
+  }
+  void prof_collect() {
+    for (int k = 0; k < kKinds; ++k) {
+      for (auto& r : prof_pending[k]) {
+        CK(cudaEventSynchronize(r.b));
+        float ms_ = 0.f;
+        CK(cudaEventElapsedTime(&ms_, r.a, r.b));
+        prof_ms[k] += ms_;
+        prof_flops[k] += r.flops;
+        ++prof_launches[k];
+        prof_free.push_back(r.a);
+        prof_free.push_back(r.b);
+      }
+      prof_pending[k].clear();
+    }
+  }
+  static double qr_flops(int m, int n) {  // complex Householder QR: 8(m n^2 - n^3/3), m >= n
+    const double a = std::max(m, n), b = std::min(m, n);
+    return 8.0 * (a * b * b - b * b * b / 3.0);
+  }
+
   // host-side statistics of the last factorize_solve (see aifmm_stats)
   double st_sync_ms = 0, st_compress_ms = 0, st_elim_ms = 0, st_back_ms = 0, st_pending_ms = 0;
   long st_syncs = 0, st_compress = 0, st_apicalls = 0;
@@ -1675,6 +1752,7 @@ struct aifmm_problem {
       pool.defer_free(db, bytes);
     }
     sync();
+    prof_collect();
     pool.commit_frees();
     launches_fs = launches_ - l0;
     ms[3] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -2048,6 +2126,25 @@ aifmm_status aifmm_launch_counts(const aifmm_problem* p, long* factor_solve, lon
   *factor_solve = p->launches_fs;
   *assemble = p->launches_asm;
   return AIFMM_OK;
+}
+
+aifmm_status aifmm_kernel_profile(aifmm_problem* p, int kind, int enable) {
+  if (!p || kind < 0 || kind >= aifmm_problem::kKinds) return AIFMM_ERR_ARG;
+  p->prof_on[kind] = enable != 0;
+  p->prof_launches[kind] = 0;
+  p->prof_ms[kind] = 0;
+  p->prof_flops[kind] = 0;
+  return AIFMM_OK;
+}
+
+aifmm_status aifmm_kernel_profile_read(aifmm_problem* p, int kind, long* launches, double* ms, double* flops) {
+  if (!p || !launches || !ms || !flops || kind < 0 || kind >= aifmm_problem::kKinds) return AIFMM_ERR_ARG;
+  return guard(p, [&] {
+    p->prof_collect();
+    *launches = p->prof_launches[kind];
+    *ms = p->prof_ms[kind];
+    *flops = p->prof_flops[kind];
+  });
 }
 
 aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n) {

@@ -134,6 +134,11 @@ aifmm_status aifmm_box_skeleton(aifmm_problem* p, int level, int box, int which,
 aifmm_status aifmm_phase_times(const aifmm_problem* p, double* ms);
 /* Number of kernel launches issued by the last factorize_solve and by the last assemble. */
 aifmm_status aifmm_launch_counts(const aifmm_problem* p, long* factor_solve, long* assemble);
+/* CUDA-event timing of one kind of kernel launch (0 QR factorisation, 1 QR solve,
+ * 2 GEMM) on the handle's stream while enabled; reading returns the launches, the
+ * summed device time (ms) and the summed algorithmic flops since it was enabled. */
+aifmm_status aifmm_kernel_profile(aifmm_problem* p, int kind, int enable);
+aifmm_status aifmm_kernel_profile_read(aifmm_problem* p, int kind, long* launches, double* ms, double* flops);
 /* Host-side statistics of the last factorize_solve: [0] ms waiting in stream syncs,
  * [1] number of syncs, [2] ms in pending-pair handling (recompression), [3] ms in the
  * per-box elimination, [4] ms in back substitution, [5] recompressions, [6] total ms,
