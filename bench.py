@@ -197,6 +197,8 @@ def main():
     ap.add_argument("--depth", type=int, default=WORKLOAD["depth"], help="override the tree depth (diagnostics)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")
+    ap.add_argument("--no-kernel-profile", action="store_true",
+                    help="skip the extra event-instrumented step that feeds the roofline (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -257,9 +259,6 @@ def main():
     for _ in range(args.warmup):
         step(False)
     fp64_peak = fp64_peak_tflops(device) if rank == 0 else None
-    kinds = {0: "qr_factor", 1: "qr_solve", 2: "gemm"}
-    for kd in kinds:
-        T.kernel_profile(kd, True)
     clocks = ClockSampler(device)
     clocks.start()
     barrier()
@@ -277,9 +276,6 @@ def main():
     ev1.record(stream)
     barrier()
     clk = clocks.stop()
-    prof = {kinds[kd]: T.kernel_profile_read(kd) for kd in kinds}
-    for kd in kinds:
-        T.kernel_profile(kd, False)
     t_dev = ev0.elapsed_time(ev1) / 1e3
     if pg is not None:
         tt = torch.tensor([t_dev], device=f"cuda:{device}")
@@ -302,8 +298,20 @@ def main():
             tt = torch.tensor([t_e2e], device=f"cuda:{device}")
             pg.all_reduce(tt, op=pg.ReduceOp.MAX)
             t_e2e = float(tt.item())
-    x = x_pin.numpy().view(np.complex128).reshape(NRHS, N)
+    x = (x_pin if t_e2e is not None else x_dev.cpu()).numpy().view(np.complex128).reshape(NRHS, N)
     finite = bool(np.isfinite(x).all())
+    # one more step, untimed, with CUDA events around every launch of the dense
+    # kernels: per-kernel durations and algorithmic flops for the roofline
+    kinds = {0: "qr_factor", 1: "qr_solve", 2: "gemm"}
+    prof = None
+    if not args.no_kernel_profile:
+        for kd in kinds:
+            T.kernel_profile(kd, True)
+        step(False)
+        torch.cuda.synchronize(device)
+        prof = {kinds[kd]: T.kernel_profile_read(kd) for kd in kinds}
+        for kd in kinds:
+            T.kernel_profile(kd, False)
     if rank == 0:
         peaks = measured_peaks()
         line = {
@@ -325,7 +333,7 @@ def main():
         }
         if not args.no_cpu_baseline and ws == 1:
             line["cpu_baseline"] = cpu_baseline_sample()
-        line["roofline"] = roofline(prof, fp64_peak, t_dev)
+        line["roofline"] = roofline(prof, fp64_peak, t_dev / args.steps) if prof else None
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.barrier()
@@ -333,7 +341,7 @@ def main():
 
 
 def roofline(prof, fp64_peak, t_dev):
-    """Dominant kernel of the timed steps (by CUDA-event device time on the solver's
+    """Dominant kernel of one event-instrumented step (by CUDA-event device time on the solver's
     stream): algorithmic flops per launch / average launch duration, against the
     FP64 peak measured above (cuBLAS DGEMM; MEASURED_PEAKS.json has no FP64 figure)."""
     name, (n, ms, fl) = max(prof.items(), key=lambda kv: kv[1][1])
