@@ -13,6 +13,7 @@
 //    (get_L2P_P2M_box, :1105-1128).
 //  * Batched GEMM / GEAM / Frobenius norms.
 // One CTA per factorisation; everything else is batched over descriptor lists.
+#include <algorithm>
 #include <cfloat>
 #include "kernels.h"
 #include "entry.cuh"
@@ -185,170 +186,196 @@ __global__ void __launch_bounds__(kT) qr_factor_kernel(const QRJob* __restrict__
   qr_factor_body(J, J.a, J.lda, J.norms, J.norms + J.n, J.perm);
 }
 
-// Jobs whose matrix fits in shared memory.  Each thread owns whole columns
-// (j = tid, tid + kT, ...): dot products, updates and norm downdates run down
-// its own columns without reductions; warp 0 builds the reflector; three
-// barriers per pivot step.  Same arithmetic order per column as the oracle.
+// Jobs whose matrix fits in shared memory, one barrier per pivot step.
+// The matrix sits in shared memory by original column ("slot"); a column swap
+// only exchanges the positions that two slots carry.  Each pivot step:
+//   1. every warp selects the pivot from the shared norms/positions and builds
+//      the reflector from the pivot column into its own buffer (all warps get the
+//      same bits: same data, same reduction order), so no warp waits for another;
+//   2. warp (k mod warps) writes the finished pivot column -- R above, beta on,
+//      the reflector below the diagonal -- straight to global memory;
+//   3. the four lanes of a group apply the reflector to each column the group
+//      owns (slots g, g + 64, ...; rows interleaved over the lanes) and downdate
+//      its norm;
+//   4. one barrier.
+// Norms and positions are double-buffered by step parity, so a warp running
+// ahead never changes what a slower warp is still scanning.  Columns left at
+// positions >= min(m, n) are written out at the end.
+// Arithmetic: pivot ties as in qr_factor_body; the reflector scalars tau and
+// 1/(a_kk - beta) come from one division; the norm downdate of LAPACK Working
+// Note 176 is evaluated without divisions -- with T = (nu - |r|)(nu + |r|) (the
+// LAWN quantity (1 - (|r|/nu)^2) times nu^2), the column is recomputed when
+// T <= sqrt(eps) nd^2 and otherwise nu becomes sqrt(T).
+constexpr int kQrGroups = kT / 4;
+__host__ __device__ __forceinline__ int qr_smem_ld(int m) { return m + ((12 - (m & 7)) & 7); }  // ld = 4 (mod 8)
+
 __global__ void __launch_bounds__(kT) qr_factor_smem_kernel(const QRJob* __restrict__ jobs) {
-  extern __shared__ double2 smem[];
-  __shared__ int s_big;
-  __shared__ double2 s_tau;
-  __shared__ double s_beta;
+  extern __shared__ double2 qsm[];
   const QRJob J = jobs[blockIdx.x];
   const int m = J.m, n = J.n, size = min(m, n);
-  const int tid = threadIdx.x, lane = tid & 31;
-  // odd leading dimension: threads walking their own columns hit distinct banks
-  const int ld = m | 1;
-  double2* A = smem;  // m x n
-  double* nu = reinterpret_cast<double*>(A + (size_t)ld * n);
-  double* nd = nu + n;
-  double2* wcol = reinterpret_cast<double2*>(nd + n);  // v^H a_j of the current step
-  int* perm = reinterpret_cast<int*>(wcol + n);
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, p = tid & 3, g = tid >> 2;
+  const int ld = qr_smem_ld(m);
+  const unsigned full = 0xffffffffu, gm = 0xfu << (lane & ~3);
+  double2* A = qsm;                                              // ld x n, by slot
+  double2* V = A + (size_t)ld * n;                               // kW x m: each warp's reflector
+  double* snu2 = reinterpret_cast<double*>(V + (size_t)kW * m);  // 2 x n: norms, by step parity
+  double* snd = snu2 + 2 * n;                                    // n: norms at the last recompute
+  double* srd = snd + n;                                         // size: |R_kk|
+  int* spos2 = reinterpret_cast<int*>(srd + size);               // 2 x n: positions, by step parity
   for (int e = tid; e < m * n; e += kT) {
     const int i = e % m, j = e / m;
     A[i + (size_t)j * ld] = J.a[i + (size_t)j * J.lda];
   }
-  for (int j = tid; j < n; j += kT) perm[j] = j;
   __syncthreads();
-  for (int j = tid; j < n; j += kT) {
-    double sq = 0.0;
-    const double2* col = A + (size_t)j * ld;
-    for (int i = 0; i < m; ++i) sq += cabs2(col[i]);
-    nu[j] = sqrt(sq);
-    nd[j] = nu[j];
+  for (int s = g; s < n; s += kQrGroups) {
+    const double2* col = A + (size_t)s * ld;
+    double q = 0.0;
+    for (int i = p; i < m; i += 4) q += cabs2(col[i]);
+    q += __shfl_xor_sync(gm, q, 1);
+    q += __shfl_xor_sync(gm, q, 2);
+    if (p == 0) { snu2[s] = snd[s] = sqrt(q); spos2[s] = s; }
   }
   __syncthreads();
+  const int nscan = (n + 31) >> 5;
   double maxnorm = 0.0;
-  for (int j = 0; j < n; ++j) maxnorm = fmax(maxnorm, nu[j]);
+  for (int q = 0; q < nscan; ++q) { const int s = lane + 32 * q; if (s < n) maxnorm = fmax(maxnorm, snu2[s]); }
+  for (int o = 16; o > 0; o >>= 1) maxnorm = fmax(maxnorm, __shfl_xor_sync(full, maxnorm, o));
   const double eps = DBL_EPSILON;
   const double thr_helper = m > 0 ? (maxnorm * eps) * (maxnorm * eps) / m : 0.0;
   const double downdate_thr = sqrt(eps);
+  double2* vw = V + (size_t)w * m;
   int nzp = size;
   double maxpivot = 0.0;
   for (int k = 0; k < size; ++k) {
-    // pivot (warp 0): largest norm among k..n-1, first index within the tie tolerance
-    if (tid < 32) {
-      double mx = 0.0;
-      for (int j = k + lane; j < n; j += 32) mx = fmax(mx, nu[j]);
-      for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      const double cut = mx * (1.0 - kPivotTie);
-      int first = 0x7fffffff;
-      for (int j = k + lane; j < n; j += 32) if (nu[j] >= cut) { first = j; break; }
-      for (int o = 16; o > 0; o >>= 1) first = min(first, __shfl_xor_sync(0xffffffffu, first, o));
-      if (lane == 0) s_big = first >= n ? k : first;
-    }
-    __syncthreads();
-    const int big = s_big;
-    if (nzp == size && nu[big] * nu[big] < thr_helper * (double)(m - k)) nzp = k;
-    // swap columns k and big (warp 0), then the reflector for A(k:m, k) (warp 0)
-    if (tid < 32) {
-      if (big != k) {
-        for (int i = lane; i < m; i += 32) {
-          double2 t = A[i + (size_t)k * ld];
-          A[i + (size_t)k * ld] = A[i + (size_t)big * ld];
-          A[i + (size_t)big * ld] = t;
-        }
-        if (lane == 0) {
-          double t = nu[k]; nu[k] = nu[big]; nu[big] = t;
-          t = nd[k]; nd[k] = nd[big]; nd[big] = t;
-          int p = perm[k]; perm[k] = perm[big]; perm[big] = p;
-        }
-        __syncwarp();
+    const double* snu = snu2 + (k & 1) * n;
+    const int* spos = spos2 + (k & 1) * n;
+    double* snu_n = snu2 + ((k + 1) & 1) * n;
+    int* spos_n = spos2 + ((k + 1) & 1) * n;
+    // 1. pivot: largest norm at positions >= k, the first position within the
+    //    tie tolerance.  Norms are non-negative: their bit patterns order like
+    //    their values, so the maximum is two unsigned warp reductions.
+    unsigned hi = 0, lo = 0;
+    for (int q = 0; q < nscan; ++q) {
+      const int s = lane + 32 * q;
+      if (s < n && spos[s] >= k) {
+        const double v = snu[s];
+        const unsigned h = (unsigned)__double2hiint(v), l = (unsigned)__double2loint(v);
+        if (h > hi || (h == hi && l > lo)) { hi = h; lo = l; }
       }
-      double tail = 0.0;
-      for (int i = k + 1 + lane; i < m; i += 32) tail += cabs2(A[i + (size_t)k * ld]);
-      tail = warp_sum(tail);
-      const double2 c0 = A[k + (size_t)k * ld];
-      double beta;
-      double2 t;
-      if (tail <= DBL_MIN && c0.y * c0.y <= DBL_MIN) {
-        beta = c0.x;
-        t = make_double2(0.0, 0.0);
-        for (int i = k + 1 + lane; i < m; i += 32) A[i + (size_t)k * ld] = make_double2(0.0, 0.0);
+    }
+    const unsigned mh = __reduce_max_sync(full, hi);
+    const unsigned ml = __reduce_max_sync(full, hi == mh ? lo : 0u);
+    const double cut = __hiloint2double((int)mh, (int)ml) * (1.0 - kPivotTie);
+    unsigned key = 0xffffffffu;
+    for (int q = 0; q < nscan; ++q) {
+      const int s = lane + 32 * q;
+      if (s < n) {
+        const int ps = spos[s];
+        if (ps >= k && snu[s] >= cut) key = min(key, (unsigned)ps * 1024u + (unsigned)s);
+      }
+    }
+    key = __reduce_min_sync(full, key);
+    const int big = (int)(key >> 10), bslot = (int)(key & 1023u);
+    const double nub = snu[bslot];
+    if (nzp == size && nub * nub < thr_helper * (double)(m - k)) nzp = k;
+    //    reflector for the pivot column, rows k..m-1
+    const double2* pc = A + (size_t)bslot * ld;
+    double tail = 0.0;
+    for (int i = k + 1 + lane; i < m; i += 32) tail += cabs2(pc[i]);
+    for (int o = 16; o > 0; o >>= 1) tail += __shfl_xor_sync(full, tail, o);
+    const double2 c0 = pc[k];
+    double beta;
+    double2 t;
+    if (tail <= DBL_MIN && c0.y * c0.y <= DBL_MIN) {
+      beta = c0.x;
+      t = make_double2(0.0, 0.0);
+      for (int i = k + 1 + lane; i < m; i += 32) vw[i] = make_double2(0.0, 0.0);
+    } else {
+      beta = sqrt(cabs2(c0) + tail);
+      if (c0.x >= 0.0) beta = -beta;
+      const double2 den = make_double2(c0.x - beta, c0.y);
+      const double dd = cabs2(den);
+      const double prod = beta * dd;
+      double ib, idd;  // 1/beta, 1/|den|^2
+      if (fabs(prod) > 1e-290 && fabs(prod) < 1e290) {
+        const double q = 1.0 / prod;
+        ib = dd * q;
+        idd = beta * q;
       } else {
-        beta = sqrt(cabs2(c0) + tail);
-        if (c0.x >= 0.0) beta = -beta;
-        const double2 den = make_double2(c0.x - beta, c0.y);
-        t = cconj(cdiv(make_double2(beta - c0.x, -c0.y), make_double2(beta, 0.0)));
-        const double2 rden = cdiv(make_double2(1.0, 0.0), den);
-        for (int i = k + 1 + lane; i < m; i += 32) A[i + (size_t)k * ld] = cmul(A[i + (size_t)k * ld], rden);
+        ib = 1.0 / beta;
+        idd = 1.0 / dd;
       }
-      __syncwarp();
-      if (lane == 0) { A[k + (size_t)k * ld] = make_double2(beta, 0.0); s_tau = t; s_beta = beta; J.tau[k] = t; }
+      t = make_double2((beta - c0.x) * ib, c0.y * ib);        // conj((beta - a_kk) / beta)
+      const double2 rden = make_double2(den.x * idd, -den.y * idd);  // 1 / (a_kk - beta)
+      for (int i = k + 1 + lane; i < m; i += 32) vw[i] = cmul(pc[i], rden);
     }
-    __syncthreads();
-    const double2 t = s_tau;
-    maxpivot = fmax(maxpivot, fabs(s_beta));
-    // apply G = I - t v v^H to columns k+1..n-1: dot products with 4 threads per
-    // column, the rank-1 update over all threads, norm downdates per column
-    const double2* v = A + (size_t)k * ld;
-    const int ncol = n - k - 1;
-    for (int base = 0; base < ncol; base += kT / 4) {
-      const int cj = base + (tid >> 2), part = tid & 3;
-      double2 sdot = make_double2(0.0, 0.0);
-      if (cj < ncol) {
-        const double2* col = A + (size_t)(k + 1 + cj) * ld;
-        for (int i = k + 1 + part; i < m; i += 4) sdot = cfmac(v[i], col[i], sdot);
-      }
-      sdot.x += __shfl_xor_sync(0xffffffffu, sdot.x, 1); sdot.y += __shfl_xor_sync(0xffffffffu, sdot.y, 1);
-      sdot.x += __shfl_xor_sync(0xffffffffu, sdot.x, 2); sdot.y += __shfl_xor_sync(0xffffffffu, sdot.y, 2);
-      if (cj < ncol && part == 0) wcol[cj] = cadd(A[k + (size_t)(k + 1 + cj) * ld], sdot);
+    maxpivot = fmax(maxpivot, fabs(beta));
+    __syncwarp();
+    // 2. the finished pivot column goes to position k
+    if (w == (k & (kW - 1))) {
+      double2* out = J.a + (size_t)k * J.lda;
+      for (int i = lane; i < m; i += 32) out[i] = i < k ? pc[i] : (i == k ? make_double2(beta, 0.0) : vw[i]);
+      if (lane == 0) { J.tau[k] = t; J.perm[k] = bslot; srd[k] = fabs(beta); }
     }
-    __syncthreads();
-    {
-      const int rows = m - k;
-      const long tot = (long)rows * ncol;
-      for (long e0 = tid; e0 < tot; e0 += 4L * kT) {
-        double2 a[4], f[4];
-        int ii[4], jj[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const long e = e0 + (long)u * kT;
-          ii[u] = -1;
-          if (e < tot) {
-            ii[u] = k + (int)(e % rows);
-            jj[u] = (int)(e / rows);
-            a[u] = A[ii[u] + (size_t)(k + 1 + jj[u]) * ld];
-            f[u] = ii[u] == k ? t : cmul(t, v[ii[u]]);
+    // 3. G = I - t v v^H on the columns at positions > k; norm downdates
+    for (int s = g; s < n; s += kQrGroups) {
+      int ps = spos[s];
+      if (ps == big) ps = k;
+      else if (ps == k) ps = big;
+      if (ps > k) {
+        double2* col = A + (size_t)s * ld;
+        const int i0 = k + 1 + ((p - (k + 1)) & 3);  // this lane's first row below k
+        double2 d0 = make_double2(0.0, 0.0), d1 = make_double2(0.0, 0.0);
+        int i = i0;
+        for (; i + 4 < m; i += 8) { d0 = cfmac(vw[i], col[i], d0); d1 = cfmac(vw[i + 4], col[i + 4], d1); }
+        if (i < m) d0 = cfmac(vw[i], col[i], d0);
+        double2 d = cadd(d0, d1);
+        d.x += __shfl_xor_sync(gm, d.x, 1); d.y += __shfl_xor_sync(gm, d.y, 1);
+        d.x += __shfl_xor_sync(gm, d.x, 2); d.y += __shfl_xor_sync(gm, d.y, 2);
+        const double2 akj = col[k];
+        const double2 tw = cmul(t, cadd(akj, d));
+        for (int r = i0; r < m; r += 4) col[r] = csub(col[r], cmul(vw[r], tw));
+        const double2 rkj = csub(akj, tw);
+        __syncwarp(gm);
+        if (p == 0) col[k] = rkj;
+        double nu = snu[s], nd = snd[s];
+        if (nu != 0.0) {
+          const double ar = sqrt(cabs2(rkj));
+          double tt = (nu - ar) * (nu + ar);
+          if (tt < 0.0) tt = 0.0;
+          if (tt <= downdate_thr * (nd * nd)) {
+            double q = 0.0;
+            for (int r = i0; r < m; r += 4) q += cabs2(col[r]);
+            q += __shfl_xor_sync(gm, q, 1);
+            q += __shfl_xor_sync(gm, q, 2);
+            nd = sqrt(q);
+            nu = nd;
+          } else {
+            nu = sqrt(tt);
           }
         }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (ii[u] >= 0) A[ii[u] + (size_t)(k + 1 + jj[u]) * ld] = csub(a[u], cmul(f[u], wcol[jj[u]]));
+        if (p == 0) { snu_n[s] = nu; snd[s] = nd; }
       }
-    }
-    __syncthreads();
-    for (int j = k + 1 + tid; j < n; j += kT) {
-      double2* col = A + (size_t)j * ld;
-      const double upd = nu[j];
-      if (upd != 0.0) {
-        double tmp = cabsd(col[k]) / upd;
-        tmp = (1.0 + tmp) * (1.0 - tmp);
-        if (tmp < 0.0) tmp = 0.0;
-        const double rr = upd / nd[j];
-        const double tmp2 = tmp * rr * rr;
-        if (tmp2 <= downdate_thr) {
-          double ss = 0.0;
-          for (int r = k + 1; r < m; ++r) ss += cabs2(col[r]);
-          nd[j] = sqrt(ss);
-          nu[j] = nd[j];
-        } else {
-          nu[j] = upd * sqrt(tmp);
-        }
-      }
+      if (p == 0) spos_n[s] = ps;
     }
     __syncthreads();
   }
-  for (int e = tid; e < m * n; e += kT) {
-    const int i = e % m, j = e / m;
-    J.a[i + (size_t)j * J.lda] = A[i + (size_t)j * ld];
+  // 4. columns that were never pivots (positions >= size)
+  const int* spos = spos2 + (size & 1) * n;
+  for (int s = g; s < n; s += kQrGroups) {
+    const int ps = spos[s];
+    if (ps >= size) {
+      const double2* col = A + (size_t)s * ld;
+      double2* out = J.a + (size_t)ps * J.lda;
+      for (int i = p; i < m; i += 4) out[i] = col[i];
+      if (p == 0) J.perm[ps] = s;
+    }
   }
-  for (int j = tid; j < n; j += kT) J.perm[j] = perm[j];
   if (tid == 0) {
     const double thr = J.thr > 0.0 ? J.thr : (double)size * eps;
     const double pre = fabs(maxpivot) * thr;
     int rk = 0;
-    for (int i = 0; i < nzp; ++i) rk += (cabsd(A[i + (size_t)i * ld]) > pre);
+    for (int i = 0; i < nzp; ++i) rk += (srd[i] > pre);
     J.info[0] = nzp;
     J.info[1] = rk;
     if (J.maxpiv) J.maxpiv[0] = maxpivot;
@@ -833,8 +860,9 @@ int aifmm_launch_qr_solve_warp(const SolveJob* d_jobs, const int* d_cta_off, int
 }
 
 size_t aifmm_qr_smem_bytes(int m, int n) {
-  return sizeof(double2) * (size_t)(m | 1) * n + sizeof(double) * 2 * (size_t)n + sizeof(double2) * (size_t)n +
-         sizeof(int) * (size_t)n + 64;
+  if (n > 1024) return ~size_t(0);  // pivot keys hold a column index below 1024
+  return sizeof(double2) * ((size_t)qr_smem_ld(m) * n + (size_t)kW * m) +
+         sizeof(double) * (3 * (size_t)n + (size_t)std::min(m, n)) + sizeof(int) * 2 * (size_t)n;
 }
 int aifmm_launch_qr_factor_smem(const QRJob* d_jobs, int njobs, size_t smem, cudaStream_t s) {
   if (njobs <= 0) return 0;
