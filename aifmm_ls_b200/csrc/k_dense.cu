@@ -401,11 +401,15 @@ __global__ void __launch_bounds__(kT) qr_solve_warp_kernel(const SolveJob* __res
   const int ldf = m | 1;
   double2* F = fsm;                      // m x nzp, ld = m|1
   double2* tau = fsm + (size_t)ldf * nzp;
+  double2* rinv = tau + nzp;             // 1 / R_kk, so that back substitution only multiplies
   for (int e = threadIdx.x; e < m * nzp; e += kT) {
     const int i = e % m, j = e / m;
     F[i + (size_t)j * ldf] = J.qr[i + (size_t)j * J.ldq];
   }
-  for (int k = threadIdx.x; k < nzp; k += kT) tau[k] = J.tau[k];
+  for (int k = threadIdx.x; k < nzp; k += kT) {
+    tau[k] = J.tau[k];
+    rinv[k] = cdiv(make_double2(1.0, 0.0), J.qr[k + (size_t)k * J.ldq]);
+  }
   __syncthreads();
   if (c >= J.nrhs) return;
   double2* x = J.X + (size_t)c * J.ldx;
@@ -434,13 +438,12 @@ __global__ void __launch_bounds__(kT) qr_solve_warp_kernel(const SolveJob* __res
     for (int r = 0; r < RPL; ++r) if (r == rk) bk = b[r];
     bk.x = __shfl_sync(0xffffffffu, bk.x, ok);
     bk.y = __shfl_sync(0xffffffffu, bk.y, ok);
-    const double2 t = tau[k];
-    const double2 wv = cadd(bk, s);
+    const double2 tw = cmul(tau[k], cadd(bk, s));
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
       const int i = lane + 32 * r;
-      if (i > k && i < m) b[r] = csub(b[r], cmul(cmul(t, v[i]), wv));
-      else if (i == k) b[r] = csub(b[r], cmul(t, wv));
+      if (i > k && i < m) b[r] = csub(b[r], cmul(v[i], tw));
+      else if (i == k) b[r] = csub(b[r], tw);
     }
   }
   for (int i = nzp - 1; i >= 0; --i) {
@@ -450,7 +453,7 @@ __global__ void __launch_bounds__(kT) qr_solve_warp_kernel(const SolveJob* __res
     for (int r = 0; r < RPL; ++r) if (r == ri) bi = b[r];
     bi.x = __shfl_sync(0xffffffffu, bi.x, oi);
     bi.y = __shfl_sync(0xffffffffu, bi.y, oi);
-    const double2 xi = cdiv(bi, F[i + (size_t)i * ldf]);
+    const double2 xi = cmul(bi, rinv[i]);
     const double2* Rc = F + (size_t)i * ldf;
 #pragma unroll
     for (int r = 0; r < RPL; ++r) {
@@ -672,7 +675,26 @@ __global__ void __launch_bounds__(kT) formq_kernel(const FormQJob* __restrict__ 
 }
 
 // ---------------------------------------------------------------- GEMM
-constexpr int TM = 32, TN = 32, TK = 16;
+// C = alpha sum_t op(A_t) op(B_t) + beta C over a list of GEMMs, one 32 x 32
+// tile of C per CTA (16 x 16 threads, 2 x 2 outputs each).  The k dimension of
+// all terms is walked in chunks of 32; the next chunk's global loads are issued
+// into registers before the current chunk is multiplied out of shared memory,
+// so one load latency hides behind each chunk's arithmetic.  Accumulation runs
+// over k in increasing order, term after term.
+constexpr int TM = 32, TN = 32, TK = 32;
+__device__ __forceinline__ void gemm_fetch(const GemmTerm& T, int k0, int row0, int col0, int m, int n,
+                                           double2 (&ra)[4], double2 (&rb)[4]) {
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int e = threadIdx.x + 256 * u;
+    const int kk = e / TM, ii = e % TM, gi = row0 + ii, gk = k0 + kk;
+    ra[u] = make_double2(0.0, 0.0);
+    if (gi < m && gk < T.k) ra[u] = T.opA ? cconj(T.A[gk + (size_t)gi * T.lda]) : T.A[gi + (size_t)gk * T.lda];
+    const int jj = e / TK, kb = e % TK, gj = col0 + jj, gkb = k0 + kb;
+    rb[u] = make_double2(0.0, 0.0);
+    if (gj < n && gkb < T.k) rb[u] = T.opB ? cconj(T.B[gj + (size_t)gkb * T.ldb]) : T.B[gkb + (size_t)gj * T.ldb];
+  }
+}
 __global__ void __launch_bounds__(256) gemm_kernel(const GemmDesc* __restrict__ ds, const GemmTerm* __restrict__ terms,
                                                    const int* __restrict__ tile_off, int nd) {
   const int bid = blockIdx.x;
@@ -684,39 +706,44 @@ __global__ void __launch_bounds__(256) gemm_kernel(const GemmDesc* __restrict__ 
   const int tm = t % tiles_m, tn = t / tiles_m;
   __shared__ double2 As[TK][TM + 1];
   __shared__ double2 Bs[TK][TN + 1];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads, 2 x 2 outputs each
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   double2 acc[2][2];
   for (int a = 0; a < 2; ++a) for (int b = 0; b < 2; ++b) acc[a][b] = make_double2(0.0, 0.0);
   const int row0 = tm * TM, col0 = tn * TN;
-  for (int t_ = 0; t_ < D.nterms; ++t_) {
-  const GemmTerm T = terms[D.term0 + t_];
-  for (int k0 = 0; k0 < T.k; k0 += TK) {
-    for (int e = threadIdx.x; e < TK * TM; e += 256) {
-      int kk = e / TM, ii = e % TM;
-      int gi = row0 + ii, gk = k0 + kk;
-      double2 v = make_double2(0.0, 0.0);
-      if (gi < D.m && gk < T.k) v = T.opA ? cconj(T.A[gk + (size_t)gi * T.lda]) : T.A[gi + (size_t)gk * T.lda];
-      As[kk][ii] = v;
-    }
-    for (int e = threadIdx.x; e < TK * TN; e += 256) {
-      int jj = e / TK, kk = e % TK;
-      int gj = col0 + jj, gk = k0 + kk;
-      double2 v = make_double2(0.0, 0.0);
-      if (gj < D.n && gk < T.k) v = T.opB ? cconj(T.B[gj + (size_t)gk * T.ldb]) : T.B[gk + (size_t)gj * T.ldb];
-      Bs[kk][jj] = v;
+  int tt = 0, k0 = 0;
+  GemmTerm T{};
+  bool have = false;
+  for (; tt < D.nterms; ++tt) { T = terms[D.term0 + tt]; if (T.k > 0) { have = true; break; } }
+  double2 ra[4], rb[4];
+  if (have) gemm_fetch(T, k0, row0, col0, D.m, D.n, ra, rb);
+  while (have) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = threadIdx.x + 256 * u;
+      As[e / TM][e % TM] = ra[u];
+      Bs[e % TK][e / TK] = rb[u];
     }
     __syncthreads();
+    // issue the next chunk's loads (possibly the next term's) before the arithmetic
+    k0 += TK;
+    bool next = true;
+    if (k0 >= T.k) {
+      next = false;
+      k0 = 0;
+      for (++tt; tt < D.nterms; ++tt) { T = terms[D.term0 + tt]; if (T.k > 0) { next = true; break; } }
+    }
+    if (next) gemm_fetch(T, k0, row0, col0, D.m, D.n, ra, rb);
 #pragma unroll
     for (int kk = 0; kk < TK; ++kk) {
-      double2 a0 = As[kk][ty], a1 = As[kk][ty + 16];
-      double2 b0 = Bs[kk][tx], b1 = Bs[kk][tx + 16];
+      const double2 a0 = As[kk][ty], a1 = As[kk][ty + 16];
+      const double2 b0 = Bs[kk][tx], b1 = Bs[kk][tx + 16];
       acc[0][0] = cfma(a0, b0, acc[0][0]);
       acc[0][1] = cfma(a0, b1, acc[0][1]);
       acc[1][0] = cfma(a1, b0, acc[1][0]);
       acc[1][1] = cfma(a1, b1, acc[1][1]);
     }
     __syncthreads();
-  }
+    have = next;
   }
   const bool zero_beta = D.beta.x == 0.0 && D.beta.y == 0.0;
   for (int a = 0; a < 2; ++a)
@@ -839,7 +866,7 @@ int aifmm_launch_qr_factor(const QRJob* d_jobs, int njobs, cudaStream_t s) {
 int aifmm_launch_qr_solve_warp(const SolveJob* d_jobs, const int* d_cta_off, int njobs, int total_ctas, int mmax,
                                int nzpmax, cudaStream_t s) {
   if (njobs <= 0 || total_ctas <= 0) return 0;
-  const size_t smem = sizeof(double2) * ((size_t)(mmax | 1) * nzpmax + nzpmax) + 64;
+  const size_t smem = sizeof(double2) * ((size_t)(mmax | 1) * nzpmax + 2 * (size_t)nzpmax) + 64;
   const int rpl = (mmax + 31) / 32;
   static bool attr[8] = {false};
   switch (rpl) {

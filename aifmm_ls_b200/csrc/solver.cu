@@ -475,7 +475,7 @@ struct aifmm_problem {
     int mmax = 1, nmax = 1;
     for (auto& j : sj) {
       const int s_ = std::min(j.m, j.n);
-      const size_t need = sizeof(double2) * ((size_t)(j.m | 1) * s_ + s_);
+      const size_t need = sizeof(double2) * ((size_t)(j.m | 1) * s_ + 2 * (size_t)s_);
       if (j.m <= 224 && need <= (size_t(200) << 10)) {
         small.push_back(j);
         mmax = std::max(mmax, j.m);
@@ -484,7 +484,7 @@ struct aifmm_problem {
         large.push_back(j);
       }
     }
-    if (sizeof(double2) * ((size_t)(mmax | 1) * nmax + nmax) > (size_t(200) << 10)) {
+    if (sizeof(double2) * ((size_t)(mmax | 1) * nmax + 2 * (size_t)nmax) > (size_t(200) << 10)) {
       // the batch's largest m and rank do not fit together: split by size
       for (auto& j : small) large.push_back(j);
       small.clear();

@@ -34,6 +34,9 @@ WORKLOAD = dict(n_cheb=6, kappa=40.0, degree=6, L=1.0, depth=7, tol_pow=10, q_ki
 NRHS = 8
 SEED = 20261203 + 1
 METRIC = "factor+solve unknowns/s (FP64, 8 RHS)"
+# DRAM bytes per launch of the QR factorisation kernel, from one ncu capture of
+# three launches in the depth-4 step (46,848 + 66,816 + 46,592 read, 0 written)
+QR_FACTOR_DRAM_BYTES_PER_LAUNCH = 53419
 FAR_ENTRY_FLOPS = 2450  # algorithmic flops of one far-field entry (121-term Graf series)
 CPU_SAMPLE_DEPTH = 4
 
@@ -348,8 +351,11 @@ def roofline(prof, fp64_peak, t_dev):
     if n == 0 or ms <= 0:
         return None
     achieved = fl / (ms * 1e-3) / 1e12
+    traffic = QR_FACTOR_DRAM_BYTES_PER_LAUNCH if name == "qr_factor" else None
     return {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-            "frac": achieved / fp64_peak if fp64_peak else None, "traffic": None,
+            "frac": achieved / fp64_peak if fp64_peak else None, "traffic": traffic,
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, mean of 3 launches of "
+                               "qr_factor_smem_kernel in the depth-4 step") if traffic else None,
             "peak_source": "FP64, measured by bench.py (cuBLAS DGEMM 8192^3, best of 5)",
             "launches": n, "avg_launch_us": 1e3 * ms / n, "algorithmic_flops_per_launch": fl / n,
             "device_time_share": 1e-3 * ms / t_dev,
