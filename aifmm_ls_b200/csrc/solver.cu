@@ -1622,62 +1622,108 @@ struct aifmm_problem {
     end_step();
   }
 
-  void back_substitution_phase() {  // F:2487-2532 (the factorisations of the elimination are reused)
+  // F:2487-2532 (the factorisations of the elimination are reused).  The
+  // reference visits the boxes of a level in decreasing order; box k reads the
+  // particles of its neighbours with a larger index (already solved) and the
+  // multipoles of the others (known from the level above).  A box therefore only
+  // waits for its larger-index neighbours: with wave(k) = 1 + max wave of those
+  // neighbours, the boxes of one wave are pairwise non-adjacent, everything they
+  // read was written by earlier waves, and each box computes exactly what the
+  // sequential order computes.  Every phase below is one batched launch per wave.
+  void back_substitution_phase() {
     for (int j = 2; j <= depth; ++j) {
-      for (int k = nBoxes[j] - 1; k >= 0; --k) {
-        Box& B = T[j][k];
-        Blk& Pkk = B.P2P[k];
-        if (Pkk.size() != 0) {
-          const int m = Pkk.r;
-          Blk rhs1 = scr(m, nrhs);
-          std::vector<std::pair<Blk, Blk>> terms;
-          for (int n = 0; n < 8; ++n) {
-            const int nn = B.nb[n];
-            if (nn == -1) continue;
-            if (!T[j][nn].elim) terms.push_back({B.P2P[nn], T[j][nn].particles});
-            else terms.push_back({B.M2P[nn], T[j][nn].multipoles});
-          }
-          copy(rhs1, B.prhs);
-          flush_geam();
-          gemm_sum(rhs1, terms, CM1, C1);
-          flush_gemm();
-          Blk t = scr(Pkk.c, nrhs);
-          solve(B.qx, rhs1, t, C1);
-          flush_solve();
-          Blk rhs2 = scr(B.P2M.r, nrhs);
-          copy(rhs2, B.multipoles);
-          flush_geam();
-          gemm(rhs2, B.P2M, 0, t, 0, CM1, C1);
-          flush_gemm();
-          Blk loc = newblk(B.L2M_f.size() != 0 ? B.L2M_f.c : 0, nrhs);
-          if (B.L2M_f.size() != 0) { solve(B.qz, rhs2, loc, C1); flush_solve(); }
-          assign(B.locals, loc);
-          Blk v = scr(m, nrhs);
-          copy(v, rhs1);
-          flush_geam();
-          gemm(v, B.L2P, 0, B.locals, 0, CM1, C1);
-          flush_gemm();
-          Blk px = newblk(Pkk.c, nrhs);
-          solve(B.qx, v, px, C1);
-          flush_solve();
-          assign(B.particles, px);
-        } else {
-          Blk px = newblk(0, nrhs);
-          assign(B.particles, px);
+      const int nbx = nBoxes[j];
+      std::vector<int> wave(nbx, 0);
+      int nw = 0;
+      for (int k = nbx - 1; k >= 0; --k) {
+        int w = 0;
+        for (int n = 0; n < 8; ++n) {
+          const int nn = T[j][k].nb[n];
+          if (nn > k) w = std::max(w, wave[nn] + 1);
         }
-        B.elim = false;
-        if (j != depth) {
-          int o = 0;
-          for (int c = 0; c < 4; ++c) {
-            Box& ch = T[j + 1][4 * k + c];
-            Blk view{B.particles.p ? B.particles.p + o : nullptr, ch.NumM, nrhs, B.particles.ld, 0};
-            ch.multipoles = view;  // a view: not owned
-            o += ch.NumM;
-          }
+        wave[k] = w;
+        nw = std::max(nw, w + 1);
+      }
+      std::vector<std::vector<int>> waves(nw);
+      for (int k = nbx - 1; k >= 0; --k) waves[wave[k]].push_back(k);
+      for (const auto& ks : waves) back_substitute_wave(j, ks);
+    }
+  }
+  void back_substitute_wave(int j, const std::vector<int>& ks) {
+    struct Work { Blk rhs1, t, rhs2, v; };
+    std::vector<Work> wk(ks.size());
+    std::vector<int> act;  // boxes with unknowns at this level
+    for (size_t q = 0; q < ks.size(); ++q)
+      if (T[j][ks[q]].P2P[ks[q]].size() != 0) act.push_back((int)q);
+    for (int q : act) {
+      Box& B = T[j][ks[q]];
+      wk[q].rhs1 = scr(B.P2P[ks[q]].r, nrhs);
+      copy(wk[q].rhs1, B.prhs);
+    }
+    flush_geam();
+    for (int q : act) {
+      Box& B = T[j][ks[q]];
+      std::vector<std::pair<Blk, Blk>> terms;
+      for (int n = 0; n < 8; ++n) {
+        const int nn = B.nb[n];
+        if (nn == -1) continue;
+        if (!T[j][nn].elim) terms.push_back({B.P2P[nn], T[j][nn].particles});
+        else terms.push_back({B.M2P[nn], T[j][nn].multipoles});
+      }
+      gemm_sum(wk[q].rhs1, terms, CM1, C1);
+    }
+    flush_gemm();
+    for (int q : act) {
+      Box& B = T[j][ks[q]];
+      wk[q].t = scr(B.P2P[ks[q]].c, nrhs);
+      solve(B.qx, wk[q].rhs1, wk[q].t, C1);
+    }
+    flush_solve();
+    for (int q : act) {
+      Box& B = T[j][ks[q]];
+      wk[q].rhs2 = scr(B.P2M.r, nrhs);
+      copy(wk[q].rhs2, B.multipoles);
+    }
+    flush_geam();
+    for (int q : act) gemm(wk[q].rhs2, T[j][ks[q]].P2M, 0, wk[q].t, 0, CM1, C1);
+    flush_gemm();
+    for (int q : act) {
+      Box& B = T[j][ks[q]];
+      Blk loc = newblk(B.L2M_f.size() != 0 ? B.L2M_f.c : 0, nrhs);
+      if (B.L2M_f.size() != 0) solve(B.qz, wk[q].rhs2, loc, C1);
+      assign(B.locals, loc);
+    }
+    flush_solve();
+    for (int q : act) {
+      wk[q].v = scr(wk[q].rhs1.r, nrhs);
+      copy(wk[q].v, wk[q].rhs1);
+    }
+    flush_geam();
+    for (int q : act) gemm(wk[q].v, T[j][ks[q]].L2P, 0, T[j][ks[q]].locals, 0, CM1, C1);
+    flush_gemm();
+    for (int q : act) {
+      Box& B = T[j][ks[q]];
+      Blk px = newblk(B.P2P[ks[q]].c, nrhs);
+      solve(B.qx, wk[q].v, px, C1);
+      assign(B.particles, px);
+    }
+    flush_solve();
+    for (size_t q = 0; q < ks.size(); ++q) {
+      const int k = ks[q];
+      Box& B = T[j][k];
+      if (B.P2P[k].size() == 0) { Blk px = newblk(0, nrhs); assign(B.particles, px); }
+      B.elim = false;
+      if (j != depth) {
+        int o = 0;
+        for (int c = 0; c < 4; ++c) {
+          Box& ch = T[j + 1][4 * k + c];
+          Blk view{B.particles.p ? B.particles.p + o : nullptr, ch.NumM, nrhs, B.particles.ld, 0};
+          ch.multipoles = view;  // a view: not owned
+          o += ch.NumM;
         }
-        end_step();
       }
     }
+    end_step();
   }
 
   void release_level_data() {

@@ -270,12 +270,14 @@ def main():
     ev0.record(stream)
     launches = 0
     asm_ms = fs_ms = 0.0
+    solver_stats = None
     for _ in range(args.steps):
         lc = step(False)
         launches += lc[0] + lc[1]
         ms = T.phase_times()
         asm_ms += ms[2]
         fs_ms += ms[3]
+        solver_stats = T.stats()
     ev1.record(stream)
     barrier()
     clk = clocks.stop()
@@ -331,6 +333,7 @@ def main():
             "gpu_launches": int(launches),
             "phases_ms_per_step": {"assemble": asm_ms / args.steps, "factorize_solve": fs_ms / args.steps,
                                    "tables_once": 1e3 * t_tables},
+            "solver_stats_last_step": solver_stats,
             "clocks": clk,
             "solution_finite": finite,
         }
