@@ -209,9 +209,7 @@ __global__ void __launch_bounds__(kT) qr_factor_kernel(const QRJob* __restrict__
 constexpr int kQrGroups = kT / 4;
 __host__ __device__ __forceinline__ int qr_smem_ld(int m) { return m + ((12 - (m & 7)) & 7); }  // ld = 4 (mod 8)
 
-__global__ void __launch_bounds__(kT) qr_factor_smem_kernel(const QRJob* __restrict__ jobs) {
-  extern __shared__ double2 qsm[];
-  const QRJob J = jobs[blockIdx.x];
+__device__ void qr_smem_body(const QRJob& J, double2* qsm) {
   const int m = J.m, n = J.n, size = min(m, n);
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, p = tid & 3, g = tid >> 2;
   const int ld = qr_smem_ld(m);
@@ -382,6 +380,137 @@ __global__ void __launch_bounds__(kT) qr_factor_smem_kernel(const QRJob* __restr
   }
 }
 
+__global__ void __launch_bounds__(kT) qr_factor_smem_kernel(const QRJob* __restrict__ jobs) {
+  extern __shared__ double2 qsm[];
+  const QRJob J = jobs[blockIdx.x];
+  qr_smem_body(J, qsm);
+}
+
+// ---------------------------------------------------------------- fused compression
+// CTA-wide building blocks on global-memory operands (written earlier by the
+// same CTA; a __syncthreads separates producer and consumer).
+
+// C (m x n, ldc) = alpha op(A) op(B) + beta C; op 1 = conjugate transpose.
+// Accumulation over k in increasing order, as gemm_kernel.
+__device__ void cta_gemm(double2* C, int ldc, int m, int n, int k, const double2* A, int lda, int opA,
+                         const double2* B, int ldb, int opB, double2 alpha, double2 beta) {
+  const bool zero_beta = beta.x == 0.0 && beta.y == 0.0;
+  for (int o = threadIdx.x; o < m * n; o += kT) {
+    const int i = o % m, jj = o / m;
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 4
+    for (int kk = 0; kk < k; ++kk) {
+      const double2 a = opA ? cconj(A[kk + (size_t)i * lda]) : A[i + (size_t)kk * lda];
+      const double2 b = opB ? cconj(B[jj + (size_t)kk * ldb]) : B[kk + (size_t)jj * ldb];
+      acc = cfma(a, b, acc);
+    }
+    double2 v = cmul(alpha, acc);
+    if (!zero_beta) v = cadd(v, cmul(beta, C[i + (size_t)jj * ldc]));
+    C[i + (size_t)jj * ldc] = v;
+  }
+}
+
+size_t aifmm_formq_smem_bytes(int m, int size, int ncols) {
+  return sizeof(double2) * ((size_t)(m | 1) * size + size + (size_t)m * ncols);
+}
+
+// Q(:, 0:ncols) = householderQ() of an m x n factor (reflectors below the
+// diagonal of qr, coefficients tau): column c is G_0^H ... G_min(c, size-1)^H e_c.
+// The factor is staged in shared memory; the four lanes of a group build one
+// column (rows interleaved), reducing the reflector dot products by shuffles.
+__device__ void cta_formq(const double2* qr, int ldq, int m, int n, const double2* tau, double2* Q, int ldQ,
+                          int ncols, double2* sm) {
+  const int size = min(m, n), ldf = m | 1;
+  const int tid = threadIdx.x, lane = tid & 31, p = tid & 3, g = tid >> 2;
+  const unsigned gm = 0xfu << (lane & ~3);
+  double2* F = sm;
+  double2* ts = F + (size_t)ldf * size;
+  double2* Qs = ts + size;
+  for (int e = tid; e < m * size; e += kT) {
+    const int i = e % m, j = e / m;
+    F[i + (size_t)j * ldf] = qr[i + (size_t)j * ldq];
+  }
+  for (int k = tid; k < size; k += kT) ts[k] = cconj(tau[k]);
+  for (int e = tid; e < m * ncols; e += kT) {
+    const int i = e % m, j = e / m;
+    Qs[e] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+  }
+  __syncthreads();
+  for (int cc = g; cc < ncols; cc += kQrGroups) {
+    double2* q = Qs + (size_t)cc * m;
+    for (int k = min(size - 1, cc); k >= 0; --k) {
+      const double2* v = F + (size_t)k * ldf;
+      const int i0 = k + 1 + ((p - (k + 1)) & 3);
+      double2 d = make_double2(0.0, 0.0);
+      for (int i = i0; i < m; i += 4) d = cfmac(v[i], q[i], d);
+      d.x += __shfl_xor_sync(gm, d.x, 1); d.y += __shfl_xor_sync(gm, d.y, 1);
+      d.x += __shfl_xor_sync(gm, d.x, 2); d.y += __shfl_xor_sync(gm, d.y, 2);
+      const double2 qk = q[k];
+      const double2 tw = cmul(ts[k], cadd(qk, d));
+      for (int i = i0; i < m; i += 4) q[i] = csub(q[i], cmul(v[i], tw));
+      __syncwarp(gm);
+      if (p == 0) q[k] = csub(qk, tw);
+      __syncwarp(gm);
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < m * ncols; e += kT) {
+    const int i = e % m, j = e / m;
+    Q[i + (size_t)j * ldQ] = Qs[e];
+  }
+}
+
+__global__ void __launch_bounds__(kT) compress_p2p_kernel(const CompressJob* __restrict__ jobs) {
+  extern __shared__ double2 csm[];
+  const CompressJob J = jobs[blockIdx.x];
+  const int m = J.m, rK = J.rK, c = J.c, rb = J.rb, n1 = rK + c;
+  const int tid = threadIdx.x;
+  const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
+  // [L2P_k | P2P_kb]
+  for (int e = tid; e < m * n1; e += kT) {
+    const int i = e % m, col = e / m;
+    J.Acol[e] = col < rK ? J.L2P[i + (size_t)col * J.ldL] : J.Pkb[i + (size_t)(col - rK) * J.ldP];
+  }
+  __syncthreads();
+  QRJob q{};
+  q.a = J.Acol; q.lda = m; q.m = m; q.n = n1; q.tau = J.tau; q.perm = J.perm; q.info = J.info; q.thr = J.tol;
+  qr_smem_body(q, csm);
+  __syncthreads();
+  const int rc = J.info[1];
+  const int ldc_ = max(rc, 1);
+  cta_formq(J.Acol, m, m, n1, J.tau, J.nL, m, rc, csm);
+  __syncthreads();
+  cta_gemm(J.Rkp, ldc_, rc, c, m, J.nL, m, 1, J.Pkb, J.ldP, 0, one, zero);   // R' = nL^H P2P_kb
+  cta_gemm(J.Rk, ldc_, rc, rK, m, J.nL, m, 1, J.L2P, J.ldL, 0, one, zero);   // R = nL^H L2P_k
+  __syncthreads();
+  // [P2M_b^H | R'^H]
+  const int n2 = rb + rc;
+  for (int e = tid; e < c * n2; e += kT) {
+    const int i = e % c, col = e / c;
+    J.Arow[e] = col < rb ? cconj(J.P2M[col + (size_t)i * J.ldM]) : cconj(J.Rkp[(col - rb) + (size_t)i * ldc_]);
+  }
+  __syncthreads();
+  q.a = J.Arow; q.lda = c; q.m = c; q.n = n2; q.info = J.info + 2;
+  qr_smem_body(q, csm);
+  __syncthreads();
+  const int rr = J.info[3];
+  const int ldr_ = max(rr, 1);
+  cta_formq(J.Arow, c, c, n2, J.tau, J.nPt, c, rr, csm);
+  __syncthreads();
+  cta_gemm(J.Rn, ldr_, rr, rb, c, J.nPt, c, 1, J.P2M, J.ldM, 1, one, zero);    // nPt^H P2M_b^H
+  cta_gemm(J.Rnp, ldr_, rr, rc, c, J.nPt, c, 1, J.Rkp, ldc_, 1, one, zero);    // nPt^H R'^H
+  cta_gemm(J.Tm, ldc_, rc, rb, rK, J.Rk, ldc_, 0, J.M2L, J.ldT, 0, one, zero);  // R M2L_kb
+  __syncthreads();
+  cta_gemm(J.M2Lo, J.ldO, rc, rr, rb, J.Tm, ldc_, 0, J.Rn, ldr_, 1, one, zero);
+  __syncthreads();
+  for (int e = tid; e < rc * rr; e += kT) {
+    const int i = e % rc, jj = e / rc;
+    double2* o = J.M2Lo + i + (size_t)jj * J.ldO;
+    *o = cadd(cconj(J.Rnp[jj + (size_t)i * ldr_]), *o);
+  }
+  if (tid == 0) { J.ranks[0] = rc; J.ranks[1] = rr; }
+}
+
 // ---------------------------------------------------------------- QR solve (warp per column, registers)
 // One warp per right-hand side; lane l holds rows l, l+32, ... of its column in
 // registers (RPL rows per lane, m <= 32*RPL).  The first nzp columns of the
@@ -468,131 +597,6 @@ __global__ void __launch_bounds__(kT) qr_solve_warp_kernel(const SolveJob* __res
   for (int r = 0; r < RPL; ++r) {
     const int i = lane + 32 * r;
     if (i < nzp) x[J.perm[i]] = cmul(J.alpha, b[r]);
-  }
-}
-
-// ---------------------------------------------------------------- QR solve (panel in shared memory)
-// One CTA per (job, panel of kSolveCols right-hand sides).  The panel B (m x
-// kSolveCols) and, when it fits, the first nzp columns of the factor live in
-// shared memory.  For each reflector, 4 threads per column form v^H b and all
-// threads apply the rank-1 update; back substitution is column oriented.
-constexpr int kSolveCols = 64;
-__global__ void __launch_bounds__(kT) qr_solve_cols_kernel(const SolveJob* __restrict__ jobs,
-                                                           const int* __restrict__ cta_off, int njobs,
-                                                           int smem_cols_cap) {
-  extern __shared__ double2 fs[];
-  __shared__ double2 wdot[kSolveCols];
-  int lo = 0, hi = njobs - 1;
-  while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (cta_off[mid] <= (int)blockIdx.x) lo = mid; else hi = mid - 1; }
-  const SolveJob J = jobs[lo];
-  const int chunk = blockIdx.x - cta_off[lo];
-  const int m = J.m, n = J.n;
-  const int nzp = J.info[0];
-  const int c0 = chunk * kSolveCols;
-  const int nc = min(kSolveCols, J.nrhs - c0);
-  const int tid = threadIdx.x;
-  if (nzp == 0) {
-    for (int e = tid; e < n * nc; e += kT) {
-      const int i = e % n, c = e / n;
-      J.X[i + (size_t)(c0 + c) * J.ldx] = make_double2(0.0, 0.0);
-    }
-    return;
-  }
-  const bool fac_in_smem = nzp <= smem_cols_cap;
-  const int ldb = m | 1;                             // odd: column-wise accesses spread over banks
-  double2* B = fs;                                   // m x kSolveCols
-  double2* F = fs + (size_t)ldb * kSolveCols;        // m x nzp
-  double2* tauS = F + (size_t)m * (fac_in_smem ? nzp : 0);
-  for (int e = tid; e < m * nc; e += kT) {
-    const int i = e % m, c = e / m;
-    B[i + (size_t)c * ldb] = J.B ? J.B[i + (size_t)(c0 + c) * J.ldb] : make_double2(i == c0 + c ? 1.0 : 0.0, 0.0);
-  }
-  if (fac_in_smem) {
-    for (int e = tid; e < m * nzp; e += kT) {
-      const int i = e % m, j = e / m;
-      F[e] = J.qr[i + (size_t)j * J.ldq];
-    }
-    for (int k = tid; k < nzp; k += kT) tauS[k] = J.tau[k];
-  }
-  __syncthreads();
-  const double2* Q = fac_in_smem ? F : J.qr;
-  const int ldq = fac_in_smem ? m : J.ldq;
-  const double2* T = fac_in_smem ? tauS : J.tau;
-  const int c = tid >> 2, part = tid & 3;  // 4 threads per column for the dots
-  for (int k = 0; k < nzp; ++k) {
-    const double2* v = Q + (size_t)k * ldq;
-    if (c < nc) {
-      const double2* col = B + (size_t)c * ldb;
-      double2 s = make_double2(0.0, 0.0);
-      for (int i = k + 1 + part; i < m; i += 4) s = cfmac(v[i], col[i], s);
-      s.x += __shfl_xor_sync(0xffffffffu, s.x, 1); s.y += __shfl_xor_sync(0xffffffffu, s.y, 1);
-      s.x += __shfl_xor_sync(0xffffffffu, s.x, 2); s.y += __shfl_xor_sync(0xffffffffu, s.y, 2);
-      if (part == 0) wdot[c] = cmul(T[k], cadd(col[k], s));  // t * (v^H b)
-    } else {
-      // keep the shuffles of the warp converged
-      double2 s = make_double2(0.0, 0.0);
-      s.x += __shfl_xor_sync(0xffffffffu, s.x, 1); s.y += __shfl_xor_sync(0xffffffffu, s.y, 1);
-      s.x += __shfl_xor_sync(0xffffffffu, s.x, 2); s.y += __shfl_xor_sync(0xffffffffu, s.y, 2);
-    }
-    __syncthreads();
-    {
-      const int rows = m - k, tot = rows * nc;
-      for (int e0 = tid; e0 < tot; e0 += 4 * kT) {
-        double2 bv[4], f[4];
-        int off[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int e = e0 + u * kT;
-          off[u] = -1;
-          if (e < tot) {
-            const int i = k + e % rows, cc = e / rows;
-            off[u] = i + cc * ldb;
-            bv[u] = B[off[u]];
-            f[u] = i == k ? wdot[cc] : cmul(v[i], wdot[cc]);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (off[u] >= 0) B[off[u]] = csub(bv[u], f[u]);
-      }
-    }
-    __syncthreads();
-  }
-  for (int i = nzp - 1; i >= 0; --i) {
-    const double2 rii = Q[i + (size_t)i * ldq];
-    for (int cc = tid; cc < nc; cc += kT) B[i + (size_t)cc * ldb] = cdiv(B[i + (size_t)cc * ldb], rii);
-    __syncthreads();
-    {
-      const int tot = i * nc;
-      for (int e0 = tid; e0 < tot; e0 += 4 * kT) {
-        double2 bv[4], f[4];
-        int off[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int e = e0 + u * kT;
-          off[u] = -1;
-          if (e < tot) {
-            const int l = e % i, cc = e / i;
-            off[u] = l + cc * ldb;
-            bv[u] = B[off[u]];
-            f[u] = cmul(Q[l + (size_t)i * ldq], B[i + cc * ldb]);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (off[u] >= 0) B[off[u]] = csub(bv[u], f[u]);
-      }
-    }
-    __syncthreads();
-  }
-  for (int e = tid; e < n * nc; e += kT) {
-    const int i = e % n, cc = e / n;
-    J.X[i + (size_t)(c0 + cc) * J.ldx] = make_double2(0.0, 0.0);
-  }
-  __syncthreads();
-  for (int e = tid; e < nzp * nc; e += kT) {
-    const int i = e % nzp, cc = e / nzp;
-    J.X[J.perm[i] + (size_t)(c0 + cc) * J.ldx] = cmul(J.alpha, B[i + (size_t)cc * ldb]);
   }
 }
 
@@ -901,20 +905,27 @@ int aifmm_launch_qr_factor_smem(const QRJob* d_jobs, int njobs, size_t smem, cud
   qr_factor_smem_kernel<<<njobs, kT, smem, s>>>(d_jobs);
   return (int)cudaGetLastError();
 }
-int aifmm_launch_qr_solve_cols(const SolveJob* d_jobs, const int* d_cta_off, int njobs, int total_ctas,
-                               int smem_cols_cap, size_t smem, cudaStream_t s) {
-  if (njobs <= 0 || total_ctas <= 0) return 0;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(qr_solve_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    attr = true;
-  }
-  qr_solve_cols_kernel<<<total_ctas, kT, smem, s>>>(d_jobs, d_cta_off, njobs, smem_cols_cap);
-  return (int)cudaGetLastError();
-}
 int aifmm_launch_qr_solve(const SolveJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s) {
   if (njobs <= 0 || total_cols <= 0) return 0;
   qr_solve_kernel<<<(total_cols + kW - 1) / kW, kT, 0, s>>>(d_jobs, d_col_off, njobs, total_cols);
+  return (int)cudaGetLastError();
+}
+size_t aifmm_compress_smem_bytes(int m, int rK, int c, int rb) {
+  const int n1 = rK + c, s1 = std::min(m, n1), n2 = rb + s1, s2 = std::min(c, n2);
+  if (m > 1024 || c > 1024) return 0;
+  size_t b = std::max(aifmm_qr_smem_bytes(m, n1), aifmm_qr_smem_bytes(c, n2));
+  b = std::max(b, aifmm_formq_smem_bytes(m, s1, s1));
+  b = std::max(b, aifmm_formq_smem_bytes(c, s2, s2));
+  return b <= (size_t(200) << 10) ? b : 0;
+}
+int aifmm_launch_compress_p2p(const CompressJob* d_jobs, int njobs, size_t smem, cudaStream_t s) {
+  if (njobs <= 0) return 0;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(compress_p2p_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    attr = true;
+  }
+  compress_p2p_kernel<<<njobs, kT, smem, s>>>(d_jobs);
   return (int)cudaGetLastError();
 }
 int aifmm_launch_formq(const FormQJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s) {

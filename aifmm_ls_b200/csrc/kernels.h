@@ -92,6 +92,28 @@ struct SkelLUJob {       // X = D^{-1} B, D = A(rows, cols) or its adjoint
   int* piv;
 };
 
+// One direction of compress_P2P (FMM2DTree_find_error.hpp:1532-1559) in one CTA:
+// column QR of [L2P_k | P2P_kb] with threshold tol -> rank rc, nL = Q(:, :rc);
+// R' = nL^H P2P_kb, R = nL^H L2P_k; row QR of [P2M_b^H | R'^H] -> rank rr,
+// nPt = Q(:, :rr); M2L' = R M2L_kb (nPt^H P2M_b^H)^H + (nPt^H R'^H)^H.
+struct CompressJob {
+  const double2* L2P; int ldL;     // m x rK
+  const double2* Pkb; int ldP;     // m x c
+  const double2* P2M; int ldM;     // rb x c
+  const double2* M2L; int ldT;     // rK x rb
+  int m, rK, c, rb;
+  double tol;
+  double2* nL;                     // out: m x rc (ld m), room for min(m, rK + c) columns
+  double2* nPt;                    // out: c x rr (ld c), room for min(c, rb + min(m, rK + c)) columns
+  double2* M2Lo; int ldO;          // out: rc x rr
+  int* ranks;                      // out: rc, rr
+  // scratch
+  double2* Acol;                   // m x (rK + c)
+  double2* Arow;                   // c x (rb + rc)
+  double2* tau; int* perm; int* info;
+  double2* Rkp; double2* Rk; double2* Rn; double2* Rnp; double2* Tm;
+};
+
 // launchers (return a cudaError_t value)
 int aifmm_launch_tables(int n_cheb, int degree, double kappa, double r, const double* gl_x, const double* gl_w,
                         const int2* basis, const double* cheb, double2* Cwork, double2* Vwork, int* status,
@@ -110,11 +132,11 @@ size_t aifmm_qr_smem_bytes(int m, int n);
 // the factor's first nzp columns must fit in shared memory
 int aifmm_launch_qr_solve_warp(const SolveJob* d_jobs, const int* d_cta_off, int njobs, int total_ctas, int mmax,
                                int nzpmax, cudaStream_t s);
+// one CTA per factorisation, the matrix in shared memory (aifmm_qr_smem_bytes)
 int aifmm_launch_qr_factor_smem(const QRJob* d_jobs, int njobs, size_t smem, cudaStream_t s);
-// panels of 64 right-hand sides per CTA in shared memory; the factor is staged
-// in shared memory when nzp <= smem_cols_cap
-int aifmm_launch_qr_solve_cols(const SolveJob* d_jobs, const int* d_cta_off, int njobs, int total_ctas,
-                               int smem_cols_cap, size_t smem, cudaStream_t s);
+// shared memory the fused compression needs for these sizes (0: does not fit)
+size_t aifmm_compress_smem_bytes(int m, int rK, int c, int rb);
+int aifmm_launch_compress_p2p(const CompressJob* d_jobs, int njobs, size_t smem, cudaStream_t s);
 int aifmm_launch_formq(const FormQJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s);
 int aifmm_launch_gemm(const GemmDesc* d, const GemmTerm* d_terms, const int* d_tile_off, int nd, int total_tiles,
                       cudaStream_t s);

@@ -1175,8 +1175,80 @@ struct aifmm_problem {
 
   // ---- recompression (F:1424-1699)
   struct CompressOut { Blk nL, nPt, M2L; };
+  // Both directions in one launch of the fused kernel (one CTA each), then one
+  // synchronisation to read the four ranks.  Returns false, having enqueued
+  // nothing, when a direction's working set does not fit in shared memory.
+  bool compress_P2P_pair_fused(int j, int k, int b, CompressOut& kb, CompressOut& bk) {
+    const int kk[2] = {k, b}, bb[2] = {b, k};
+    CompressOut* out[2] = {&kb, &bk};
+    size_t smem = 0;
+    for (int s = 0; s < 2; ++s) {
+      Box& K = T[j][kk[s]];
+      Box& Bb = T[j][bb[s]];
+      const Blk& Pkb = K.P2P[bb[s]];
+      const Blk& m2l = K.M2L[bb[s]];
+      if (Pkb.r != K.L2P.r) throw Fail(AIFMM_ERR_NUMERIC, "compress_P2P: block rows mismatch");
+      if (Bb.P2M.c != Pkb.c || m2l.r != K.L2P.c || m2l.c != Bb.P2M.r)
+        throw Fail(AIFMM_ERR_NUMERIC, "compress_P2P: block shapes");
+      const size_t need = aifmm_compress_smem_bytes(K.L2P.r, K.L2P.c, Pkb.c, Bb.P2M.r);
+      if (need == 0) return false;
+      smem = std::max(smem, need);
+    }
+    std::vector<CompressJob> jobs(2);
+    int* ranks = static_cast<int*>(scratch.get(sizeof(int) * 4));
+    int rcmax[2], rrmax[2];
+    for (int s = 0; s < 2; ++s) {
+      Box& K = T[j][kk[s]];
+      Box& Bb = T[j][bb[s]];
+      const Blk& Pkb = K.P2P[bb[s]];
+      const Blk& m2l = K.M2L[bb[s]];
+      const int m = K.L2P.r, rK = K.L2P.c, c = Pkb.c, rb = Bb.P2M.r, n1 = rK + c;
+      rcmax[s] = std::min(m, n1);
+      const int n2max = rb + rcmax[s];
+      rrmax[s] = std::min(c, n2max);
+      out[s]->nL = newblk(m, rcmax[s]);
+      out[s]->nPt = newblk(c, rrmax[s]);
+      out[s]->M2L = scr(rcmax[s], rrmax[s]);
+      CompressJob& J = jobs[s];
+      J.L2P = K.L2P.p; J.ldL = K.L2P.ld;
+      J.Pkb = Pkb.p; J.ldP = Pkb.ld;
+      J.P2M = Bb.P2M.p; J.ldM = Bb.P2M.ld;
+      J.M2L = m2l.p; J.ldT = m2l.ld;
+      J.m = m; J.rK = rK; J.c = c; J.rb = rb; J.tol = tol;
+      J.nL = out[s]->nL.p; J.nPt = out[s]->nPt.p;
+      J.M2Lo = out[s]->M2L.p; J.ldO = out[s]->M2L.ld;
+      J.ranks = ranks + 2 * s;
+      auto cg = [&](long elems) { return static_cast<double2*>(scratch.get(sizeof(double2) * std::max(1L, elems))); };
+      J.Acol = cg((long)m * n1);
+      J.Arow = cg((long)c * n2max);
+      J.tau = cg(std::max(rcmax[s], rrmax[s]));
+      J.perm = static_cast<int*>(scratch.get(sizeof(int) * std::max(1, std::max(n1, n2max))));
+      J.info = static_cast<int*>(scratch.get(sizeof(int) * 4));
+      J.Rkp = cg((long)rcmax[s] * c);
+      J.Rk = cg((long)rcmax[s] * rK);
+      J.Rn = cg((long)rrmax[s] * rb);
+      J.Rnp = cg((long)rrmax[s] * rcmax[s]);
+      J.Tm = cg((long)rcmax[s] * rb);
+    }
+    flush_all();
+    const CompressJob* dj = stage.put(jobs, st);
+    KL(aifmm_launch_compress_p2p(dj, 2, smem, st));
+    sync();
+    int rk[4];
+    CK(cudaMemcpy(rk, ranks, sizeof rk, cudaMemcpyDeviceToHost));
+    for (int s = 0; s < 2; ++s) {
+      const int rc = rk[2 * s], rr = rk[2 * s + 1];
+      if (rc < 0 || rc > rcmax[s] || rr < 0 || rr > rrmax[s]) throw Fail(AIFMM_ERR_NUMERIC, "compress_P2P: rank out of range");
+      out[s]->nL.c = rc;
+      out[s]->nPt.c = rr;
+      out[s]->M2L.r = rc;
+      out[s]->M2L.c = rr;
+    }
+    return true;
+  }
   // Both directions of compress_P2P (F:1532-1559) in lockstep: (k,b) and (b,k)
   void compress_P2P_pair(int j, int k, int b, CompressOut& kb, CompressOut& bk) {
+    if (compress_P2P_pair_fused(j, k, b, kb, bk)) return;
     int kk[2] = {k, b}, bb[2] = {b, k};
     Blk Acol[2], Rk_prime[2], Rk[2], Arow[2];
     QRF qc[2], qw[2];
