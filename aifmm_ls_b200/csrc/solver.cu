@@ -152,7 +152,7 @@ class Staging {
     size_t tot = 0;
     for (auto& p : parts) tot += (p.second + 255) & ~size_t(255);
     if (tot > cap_) throw Fail(AIFMM_ERR_NOMEM, "descriptor batch larger than the staging ring");
-    if (off_ + tot > cap_) { CK(cudaStreamSynchronize(s)); off_ = 0; }
+    if (off_ + tot > cap_) { CK(cudaDeviceSynchronize()); off_ = 0; }  // both solver streams
     std::vector<const void*> out;
     size_t o = off_;
     for (auto& p : parts) {
@@ -167,7 +167,7 @@ class Staging {
   const void* put_raw(const void* src, size_t bytes, cudaStream_t s) {
     size_t b = (bytes + 255) & ~size_t(255);
     if (b > cap_) throw Fail(AIFMM_ERR_NOMEM, "descriptor batch larger than the staging ring");
-    if (off_ + b > cap_) { CK(cudaStreamSynchronize(s)); off_ = 0; }
+    if (off_ + b > cap_) { CK(cudaDeviceSynchronize()); off_ = 0; }  // both solver streams
     memcpy(h_ + off_, src, bytes);
     CK(cudaMemcpyAsync(d_ + off_, h_ + off_, bytes, cudaMemcpyHostToDevice, s));
     const void* r = d_ + off_;
@@ -273,6 +273,10 @@ struct aifmm_problem {
   aifmm_desc d;
   int device = 0;
   cudaStream_t st = nullptr;
+  // second stream for the part of a box step that the step's recompressions do
+  // not touch; cur is the stream the batched launches go to
+  cudaStream_t st2 = nullptr, cur = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string err;
   int rank = 0, N = 0, nleaf = 0, depth = 0, nb = 0;
   double tol = 0;
@@ -377,11 +381,11 @@ struct aifmm_problem {
       for (int t = 0; t < g.nterms; ++t) fl += 8.0 * g.m * g.n * gt[g.term0 + t].k;
     if (gt.empty()) gt.push_back(GemmTerm{});
     auto ptrs = stage.put_many({{gt.data(), gt.size() * sizeof(GemmTerm)}, {gd.data(), gd.size() * sizeof(GemmDesc)},
-                                {off.data(), off.size() * sizeof(int)}}, st);
+                                {off.data(), off.size() * sizeof(int)}}, cur);
     cudaEvent_t a;
     const bool pr = prof_begin(2, a);
     KL(aifmm_launch_gemm(static_cast<const GemmDesc*>(ptrs[1]), static_cast<const GemmTerm*>(ptrs[0]),
-                         static_cast<const int*>(ptrs[2]), (int)gd.size(), tot, st));
+                         static_cast<const int*>(ptrs[2]), (int)gd.size(), tot, cur));
     if (pr) prof_end(2, a, fl);
     gd.clear(); gt.clear();
   }
@@ -399,15 +403,15 @@ struct aifmm_problem {
     std::vector<long long> off(ged.size());
     long long tot = 0;
     for (size_t i = 0; i < ged.size(); ++i) { off[i] = tot; tot += (long long)ged[i].m * ged[i].n; }
-    auto ptrs = stage.put_many({{ged.data(), ged.size() * sizeof(GeamDesc)}, {off.data(), off.size() * sizeof(long long)}}, st);
+    auto ptrs = stage.put_many({{ged.data(), ged.size() * sizeof(GeamDesc)}, {off.data(), off.size() * sizeof(long long)}}, cur);
     KL(aifmm_launch_geam(static_cast<const GeamDesc*>(ptrs[0]), static_cast<const long long*>(ptrs[1]),
-                         (int)ged.size(), tot, st));
+                         (int)ged.size(), tot, cur));
     ged.clear();
   }
   void zero(const Blk& b) {
     if (b.size() == 0) return;
-    if (b.ld == b.r) CK(cudaMemsetAsync(b.p, 0, sizeof(double2) * (size_t)b.r * b.c, st));
-    else for (int j = 0; j < b.c; ++j) CK(cudaMemsetAsync(b.p + (size_t)j * b.ld, 0, sizeof(double2) * b.r, st));
+    if (b.ld == b.r) CK(cudaMemsetAsync(b.p, 0, sizeof(double2) * (size_t)b.r * b.c, cur));
+    else for (int j = 0; j < b.c; ++j) CK(cudaMemsetAsync(b.p + (size_t)j * b.ld, 0, sizeof(double2) * b.r, cur));
   }
   // QR factorisation of A in place (threshold 0 -> Eigen default)
   void qr_prepare(QRF& f, const Blk& A, double thr, bool persistent) {
@@ -440,17 +444,17 @@ struct aifmm_problem {
       else { large.push_back(j); fl_large += qr_flops(j.m, j.n); }
     }
     if (!small.empty()) {
-      const QRJob* dq = stage.put(small, st);
+      const QRJob* dq = stage.put(small, cur);
       cudaEvent_t a;
       const bool pr = prof_begin(0, a);
-      KL(aifmm_launch_qr_factor_smem(dq, (int)small.size(), smem, st));
+      KL(aifmm_launch_qr_factor_smem(dq, (int)small.size(), smem, cur));
       if (pr) prof_end(0, a, fl_small);
     }
     if (!large.empty()) {
-      const QRJob* dq = stage.put(large, st);
+      const QRJob* dq = stage.put(large, cur);
       cudaEvent_t a;
       const bool pr = prof_begin(0, a);
-      KL(aifmm_launch_qr_factor(dq, (int)large.size(), st));
+      KL(aifmm_launch_qr_factor(dq, (int)large.size(), cur));
       if (pr) prof_end(0, a, fl_large);
     }
     qj.clear();
@@ -493,13 +497,13 @@ struct aifmm_problem {
       std::vector<int> off(small.size());
       int tot = 0;
       for (size_t i = 0; i < small.size(); ++i) { off[i] = tot; tot += (small[i].nrhs + 7) / 8; }
-      auto ptrs = stage.put_many({{small.data(), small.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}}, st);
+      auto ptrs = stage.put_many({{small.data(), small.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}}, cur);
       double fl = 0;
       for (auto& j : small) { const double mz = std::min(j.m, j.n); fl += (16.0 * j.m * mz - 4.0 * mz * mz) * j.nrhs; }
       cudaEvent_t a;
       const bool pr = prof_begin(1, a);
       KL(aifmm_launch_qr_solve_warp(static_cast<const SolveJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]),
-                                    (int)small.size(), tot, mmax, nmax, st));
+                                    (int)small.size(), tot, mmax, nmax, cur));
       if (pr) prof_end(1, a, fl);
     }
     if (!large.empty()) {
@@ -510,13 +514,13 @@ struct aifmm_problem {
         tot += large[i].nrhs;
         large[i].work = static_cast<double2*>(scratch.get(sizeof(double2) * (size_t)large[i].m * large[i].nrhs));
       }
-      auto ptrs = stage.put_many({{large.data(), large.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}}, st);
+      auto ptrs = stage.put_many({{large.data(), large.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}}, cur);
       double fl = 0;
       for (auto& j : large) { const double mz = std::min(j.m, j.n); fl += (16.0 * j.m * mz - 4.0 * mz * mz) * j.nrhs; }
       cudaEvent_t a;
       const bool pr = prof_begin(1, a);
       KL(aifmm_launch_qr_solve(static_cast<const SolveJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]),
-                               (int)large.size(), tot, st));
+                               (int)large.size(), tot, cur));
       if (pr) prof_end(1, a, fl);
     }
     sj.clear();
@@ -532,9 +536,9 @@ struct aifmm_problem {
     std::vector<int> off(fq.size());
     int tot = 0;
     for (size_t i = 0; i < fq.size(); ++i) { off[i] = tot; tot += fq[i].ncols; }
-    auto ptrs = stage.put_many({{fq.data(), fq.size() * sizeof(FormQJob)}, {off.data(), off.size() * sizeof(int)}}, st);
+    auto ptrs = stage.put_many({{fq.data(), fq.size() * sizeof(FormQJob)}, {off.data(), off.size() * sizeof(int)}}, cur);
     KL(aifmm_launch_formq(static_cast<const FormQJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]), (int)fq.size(),
-                          tot, st));
+                          tot, cur));
     fq.clear();
   }
   void flush_all() { flush_geam(); flush_qr(); flush_solve(); flush_formq(); flush_gemm(); }
@@ -556,12 +560,12 @@ struct aifmm_problem {
   bool prof_begin(int kind, cudaEvent_t& a) {
     if (!prof_on[kind]) return false;
     a = prof_event();
-    CK(cudaEventRecord(a, st));
+    CK(cudaEventRecord(a, cur));
     return true;
   }
   void prof_end(int kind, cudaEvent_t a, double flops) {
     cudaEvent_t b = prof_event();
-    CK(cudaEventRecord(b, st));
+    CK(cudaEventRecord(b, cur));
     prof_pending[kind].push_back({a, b, flops});
     if (prof_pending[kind].size() > 4096) prof_collect();
   }
@@ -609,6 +613,10 @@ struct aifmm_problem {
       throw Fail(AIFMM_ERR_ARG, "more polynomial bases than nodes per leaf");
     CK(cudaSetDevice(dev));
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    cur = st;
     rank = d.n_cheb * d.n_cheb;
     depth = d.depth;
     nleaf = 1 << (2 * depth);
@@ -645,6 +653,9 @@ struct aifmm_problem {
     cudaFree(d_iota); cudaFree(d_norms);
     if (h_norms) cudaFreeHost(h_norms);
     if (st) cudaStreamDestroy(st);
+    if (st2) cudaStreamDestroy(st2);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
   }
 
   void tables_compute(int do_round) {
@@ -1008,23 +1019,66 @@ struct aifmm_problem {
     }
   }
 
+  // The part of eliminate_x that the recompressions of the same step cannot
+  // change: they touch the bases of k and of boxes well separated from k, the
+  // M2L blocks and the level above, never P2P[k][k], k's right-hand side or its
+  // blocks towards its neighbours.  So the factorisation of P2P[k][k] and its
+  // solves with those blocks run on the second stream, overlapping the
+  // recompressions and their synchronisations on the main stream.
+  struct SideX { bool on = false; Blk Xb, W[8]; };
+  SideX sx;
+  void eliminate_x_side(int j, int k) {
+    sx = SideX();
+    Box& B = T[j][k];
+    Blk& Pkk = B.P2P[k];
+    if (Pkk.size() == 0) return;
+    flush_all();
+    CK(cudaEventRecord(ev_fork, st));
+    CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+    cur = st2;
+    qr_prepare(B.qx, Pkk, 0.0, true);  // factored in place; P2P[k][k] is not read again
+    flush_qr();
+    const int m = Pkk.c;
+    sx.Xb = scr(m, nrhs);
+    solve(B.qx, B.prhs, sx.Xb, C1);
+    for (int pI = 0; pI < 8; ++pI) {
+      const int pp = B.nb[pI];
+      if (pp == -1) continue;
+      const Blk& src = T[j][pp].elim ? B.M2P[pp] : B.P2P[pp];
+      sx.W[pI] = scr(m, src.c);
+      solve(B.qx, src, sx.W[pI], C1);
+    }
+    flush_solve();
+    CK(cudaEventRecord(ev_join, st2));
+    cur = st;
+    sx.on = true;
+  }
   void eliminate_x(int j, int k) {  // F:1814-1840, 1961-2075 (and the no-QR branch :1843-1957)
     Box& B = T[j][k];
     Blk& Pkk = B.P2P[k];
     if (Pkk.size() != 0) {
-      qr_prepare(B.qx, Pkk, 0.0, true);  // factored in place; P2P[k][k] is not read again
-      flush_qr();
       const int m = Pkk.c;
-      Blk XL = scr(m, B.L2P.c), Xb = scr(m, nrhs), W[8];
-      solve(B.qx, B.L2P, XL, C1);
-      solve(B.qx, B.prhs, Xb, C1);
-      for (int pI = 0; pI < 8; ++pI) {
-        const int pp = B.nb[pI];
-        if (pp == -1) continue;
-        const Blk& src = T[j][pp].elim ? B.M2P[pp] : B.P2P[pp];
-        W[pI] = scr(m, src.c);
-        solve(B.qx, src, W[pI], C1);
+      Blk XL = scr(m, B.L2P.c), Xb, W[8];
+      if (sx.on) {
+        CK(cudaStreamWaitEvent(st, ev_join, 0));
+        Xb = sx.Xb;
+        for (int q = 0; q < 8; ++q) W[q] = sx.W[q];
+        solve(B.qx, B.L2P, XL, C1);
+      } else {
+        qr_prepare(B.qx, Pkk, 0.0, true);
+        flush_qr();
+        Xb = scr(m, nrhs);
+        solve(B.qx, B.L2P, XL, C1);
+        solve(B.qx, B.prhs, Xb, C1);
+        for (int pI = 0; pI < 8; ++pI) {
+          const int pp = B.nb[pI];
+          if (pp == -1) continue;
+          const Blk& src = T[j][pp].elim ? B.M2P[pp] : B.P2P[pp];
+          W[pI] = scr(m, src.c);
+          solve(B.qx, src, W[pI], C1);
+        }
       }
+      sx.on = false;
       flush_solve();
       { Blk t = newblk(B.P2M.r, XL.c); gemm(t, B.P2M, 0, XL, 0, CM1, C0); assign(B.L2M_f, t); }
       for (int n = 0; n < 8; ++n) {
@@ -1611,6 +1665,7 @@ struct aifmm_problem {
       if (j != depth) initialise_P2P_NonLeafLevel(j);
       for (int k = 0; k < nBoxes[j]; ++k) {
         auto tp0 = std::chrono::steady_clock::now();
+        eliminate_x_side(j, k);
         take_pending(j, k, p2p, p2l);
         for (auto& pr : p2p) {
           const int nn = pr.first, pp = pr.second;
