@@ -790,7 +790,10 @@ __global__ void __launch_bounds__(kT) norm_kernel(const NormDesc* __restrict__ d
     s += cabs2(D.A[i + (size_t)j * D.lda]);
   }
   s = block_sum(s, sh);
-  if (threadIdx.x == 0) D.out[0] = sqrt(s);
+  if (threadIdx.x == 0) {
+    D.out[0] = sqrt(s);  // may be mapped host memory
+    __threadfence_system();
+  }
 }
 
 // ---------------------------------------------------------------- skeleton LU solve

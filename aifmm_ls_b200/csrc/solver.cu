@@ -20,6 +20,7 @@
 #include <map>
 #include <memory>
 #include <stdexcept>
+#include <set>
 #include <string>
 #include <utility>
 #include <vector>
@@ -300,9 +301,13 @@ struct aifmm_problem {
   // pending fill-in candidates of the last eliminated box (kind 0 = P2P, 1 = P2L)
   struct Cand { int kind, nn, pp; };
   std::vector<Cand> cands;
-  double* d_norms = nullptr;   // device norm slots
-  double* h_norms = nullptr;   // pinned copy
+  // Fill-in norm slots in mapped pinned host memory: the norm kernels write them
+  // and the host reads them once the event of their phase has completed.
+  double* d_norms = nullptr;   // device view of h_norms
+  double* h_norms = nullptr;
   int norm_cap = 0;
+  cudaEvent_t ev_norm[2] = {nullptr, nullptr};  // after the x- and z-phase norm launches
+  int ncand[2] = {0, 0};                        // candidates recorded when each event was set
   bool norms_pending = false;
 
   EntryCtx ctx() const {
@@ -591,6 +596,9 @@ struct aifmm_problem {
 
   // host-side statistics of the last factorize_solve (see aifmm_stats)
   double st_sync_ms = 0, st_compress_ms = 0, st_elim_ms = 0, st_back_ms = 0, st_pending_ms = 0;
+  // assembly split: host index lists, ACA (launch to ranks on the host),
+  // interpolative operators, M2L/P2P block entries (launch to completion)
+  double st_asm_lists_ms = 0, st_asm_aca_ms = 0, st_asm_lu_ms = 0, st_asm_blocks_ms = 0;
   long st_syncs = 0, st_compress = 0, st_apicalls = 0;
   void sync() {
     auto t0 = std::chrono::steady_clock::now();
@@ -642,16 +650,19 @@ struct aifmm_problem {
     KL(aifmm_launch_geometry(d.n_cheb, depth, d.L, d.q_kind, d.q_amp, d.q_width, d.q_radius, d_cheb, d_pts, d_q,
                              d_leafc, d_leafxy, st));
     norm_cap = 4096;
-    CK(cudaMalloc(&d_norms, sizeof(double) * norm_cap));
-    CK(cudaMallocHost(&h_norms, sizeof(double) * norm_cap));
+    CK(cudaHostAlloc(&h_norms, sizeof(double) * norm_cap, cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer(&d_norms, h_norms, 0));
+    for (auto& e : ev_norm) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     sync();
   }
   void destroy() {
     if (st) cudaStreamSynchronize(st);
+    if (st2) cudaStreamSynchronize(st2);
     pool.release_all();
     cudaFree(d_pts); cudaFree(d_q); cudaFree(d_leafc); cudaFree(d_leafxy); cudaFree(d_M); cudaFree(d_near);
-    cudaFree(d_iota); cudaFree(d_norms);
+    cudaFree(d_iota);
     if (h_norms) cudaFreeHost(h_norms);
+    for (auto& e : ev_norm) if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
     if (st2) cudaStreamDestroy(st2);
     if (ev_fork) cudaEventDestroy(ev_fork);
@@ -770,8 +781,12 @@ struct aifmm_problem {
     auto t0 = std::chrono::steady_clock::now();
     const long l0 = launches_;
     const EntryCtx cx = ctx();
+    using clk = std::chrono::steady_clock;
+    auto since = [](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
+    st_asm_lists_ms = st_asm_aca_ms = st_asm_lu_ms = st_asm_blocks_ms = 0;
     for (int j = depth; j >= 2; --j) {
       const int nbx = nBoxes[j];
+      auto ta = clk::now();
       // ---- index lists for the outgoing and incoming ACA of every box (F:1230-1336)
       std::vector<int> idx;
       struct JobIdx { long r0, c0; int n1, n2; };
@@ -839,6 +854,8 @@ struct aifmm_problem {
         if (outgoing) { drop(B.Ar); B.Ar = newblk(rmax, n2); J.out = B.Ar.p; B.Ar.ld = std::max(rmax, 1); }
         else { drop(B.Ac); B.Ac = newblk(n1, rmax); J.out = B.Ac.p; }
       }
+      st_asm_lists_ms += since(ta);
+      ta = clk::now();
       const AcaJob* dj = stage.put(jobs, st);
       KL(aifmm_launch_aca(dj, (int)jobs.size(), tol, cx, st));
       // ---- ranks and skeletons back to the host
@@ -858,6 +875,8 @@ struct aifmm_problem {
       cudaFree(d_res);
       cudaFree(d_ws);
       cudaFree(d_idx);
+      st_asm_aca_ms += since(ta);
+      ta = clk::now();
       // ---- skeletons, rank equalisation (F:1105-1113) and L2P / P2M jobs
       std::vector<int> sk;  // skeleton index lists for the LU jobs
       struct LUI { long rows, cols; };
@@ -936,7 +955,9 @@ struct aifmm_problem {
       }
       for (int k = 0; k < nbx; ++k) { Box& B = T[j][k]; drop(B.Ac); drop(B.Ar); }
       pool.commit_frees();
+      st_asm_lu_ms += since(ta);
     }
+    auto tb = clk::now();
     // ---- M2L blocks (F:1338-1361) and leaf P2P blocks (F:1729-1741)
     {
       std::vector<int> sk;
@@ -985,6 +1006,7 @@ struct aifmm_problem {
     for (int j = 2; j <= depth; ++j)
       for (int k = 0; k < nBoxes[j]; ++k) { Box& B = T[j][k]; B.NumM = B.P2M.r; B.NumL = B.L2P.c; }
     sync();
+    st_asm_blocks_ms = since(tb);
     pool.commit_frees();
     assembled = true;
     launches_asm = launches_ - l0;
@@ -1006,18 +1028,30 @@ struct aifmm_problem {
 
   void record_cand(int kind, int nn, int pp, const Blk& b) {
     if ((int)cands.size() >= norm_cap) throw Fail(AIFMM_ERR_NUMERIC, "too many fill-in candidates");
-    NormDesc n; n.A = b.p; n.lda = b.ld; n.m = b.r; n.n = b.c; n.out = d_norms + cands.size();
+    // every slot is written by a norm kernel (an empty block gives 0), so all
+    // writes to the slots are ordered by the stream
+    NormDesc n; n.A = b.p; n.lda = std::max(b.ld, 1); n.m = b.size() ? b.r : 0; n.n = b.size() ? b.c : 0;
+    n.out = d_norms + cands.size();
     cands.push_back({kind, nn, pp});
-    if (b.size() == 0) { CK(cudaMemsetAsync(n.out, 0, sizeof(double), st)); return; }
     ndv.push_back(n);
   }
-  void flush_norms() {
+  // phase 0: the norms recorded by eliminate_x; phase 1: by eliminate_z
+  void flush_norms(int phase) {
     if (!ndv.empty()) {
       const NormDesc* dn = stage.put(ndv, st);
       KL(aifmm_launch_norms(dn, (int)ndv.size(), st));
       ndv.clear();
     }
+    CK(cudaEventRecord(ev_norm[phase], st));
+    ncand[phase] = (int)cands.size();
   }
+  void wait_norms(int phase) {
+    auto t0 = std::chrono::steady_clock::now();
+    CK(cudaEventSynchronize(ev_norm[phase]));
+    st_sync_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    ++st_syncs;
+  }
+  void clear_cands() { cands.clear(); ncand[0] = ncand[1] = 0; }
 
   // The part of eliminate_x that the recompressions of the same step cannot
   // change: they touch the bases of k and of boxes well separated from k, the
@@ -1116,7 +1150,7 @@ struct aifmm_problem {
         gemm(Nn.elim ? Nn.mrhs : Nn.prhs, Xnk, 0, Xb, 0, CM1, C1);
       }
       flush_gemm();
-      flush_norms();
+      flush_norms(0);
     } else {
       // box k carries no unknowns: the reference stores uninitialised blocks whose
       // intended value (a product with an empty inner dimension) is zero
@@ -1153,7 +1187,7 @@ struct aifmm_problem {
           }
         }
       }
-      flush_norms();
+      flush_norms(0);
     }
   }
 
@@ -1199,7 +1233,7 @@ struct aifmm_problem {
         gemm(Nn.elim ? Nn.mrhs : Nn.prhs, Lf, 0, Yrhs, 0, CM1, C1);
       }
       flush_gemm();
-      flush_norms();
+      flush_norms(1);
     } else {
       { Blk t = newblk(0, B.NumM); assign(B.M2L[k], t); }
       for (int n = 0; n < 8; ++n) {
@@ -1223,7 +1257,7 @@ struct aifmm_problem {
           else if (Nn.elim && !pe) { if (well_sep(j, nn, pp)) record_cand(1, nn, pp, Nn.P2L[pp]); }
         }
       }
-      flush_norms();
+      flush_norms(1);
     }
   }
 
@@ -1640,27 +1674,51 @@ struct aifmm_problem {
     flush_geam();
   }
 
+  // The pairs queued by the previous box step (F:2411-2438): an instance is
+  // queued when its fill-in norm exceeds 1e-10 at the time it was recorded, and
+  // only instances involving k are compressed, in the order they were queued.
+  // The x-phase norms are waited for first; a z-phase instance matters only if
+  // its pair was not already queued by an x-phase instance (a repeated pair is
+  // a no-op: its block is gone after the first compression), so the z-phase
+  // norms (the end of the previous step's chain) are waited for only then.
   void take_pending(int j, int k, std::vector<std::pair<int, int>>& p2p, std::vector<std::pair<int, int>>& p2l) {
     p2p.clear(); p2l.clear();
+    const int n = (int)cands.size();
+    auto inv = [&](int i) { return cands[i].nn == k || cands[i].pp == k; };
     bool involved = false;
-    for (auto& c : cands) if (c.nn == k || c.pp == k) { involved = true; break; }
-    if (!involved) { cands.clear(); return; }
-    if (!cands.empty()) {
-      CK(cudaMemcpyAsync(h_norms, d_norms, sizeof(double) * cands.size(), cudaMemcpyDeviceToHost, st));
-      sync();
+    for (int i = 0; i < n; ++i) if (inv(i)) { involved = true; break; }
+    if (!involved) { clear_cands(); return; }
+    const int nx = std::min(ncand[0], n);
+    std::vector<char> take(n, 0);
+    std::set<std::tuple<int, int, int>> queued;
+    bool x_inv = false;
+    for (int i = 0; i < nx; ++i) x_inv = x_inv || inv(i);
+    if (x_inv) {
+      wait_norms(0);
+      for (int i = 0; i < nx; ++i)
+        if (inv(i) && h_norms[i] > 1e-10) { take[i] = 1; queued.insert(std::make_tuple(cands[i].kind, cands[i].nn, cands[i].pp)); }
     }
-    for (size_t i = 0; i < cands.size(); ++i) {
-      if (!(h_norms[i] > 1e-10)) continue;
+    bool need_z = false;
+    for (int i = nx; i < n; ++i)
+      if (inv(i) && !queued.count(std::make_tuple(cands[i].kind, cands[i].nn, cands[i].pp))) { need_z = true; break; }
+    if (need_z) {
+      wait_norms(1);
+      for (int i = nx; i < n; ++i)
+        if (inv(i) && !queued.count(std::make_tuple(cands[i].kind, cands[i].nn, cands[i].pp)) && h_norms[i] > 1e-10)
+          take[i] = 1;
+    }
+    for (int i = 0; i < n; ++i) {
+      if (!take[i]) continue;
       if (cands[i].kind == 0) p2p.push_back({cands[i].nn, cands[i].pp});
       else p2l.push_back({cands[i].nn, cands[i].pp});
     }
-    cands.clear();
+    clear_cands();
     (void)j;
   }
 
   void eliminate_phase_efficient() {  // F:2407-2451
     std::vector<std::pair<int, int>> p2p, p2l;
-    cands.clear();
+    clear_cands();
     for (int j = depth; j >= 2; --j) {
       if (j != depth) initialise_P2P_NonLeafLevel(j);
       for (int k = 0; k < nBoxes[j]; ++k) {
@@ -1694,7 +1752,8 @@ struct aifmm_problem {
         st_pending_ms += std::chrono::duration<double, std::milli>(tp1 - tp0).count();
         st_elim_ms += std::chrono::duration<double, std::milli>(tp2 - tp1).count();
       }
-      cands.clear();  // pending pairs never cross a level
+      sync();
+      clear_cands();  // pending pairs never cross a level
     }
     solve_base(2);
   }
@@ -2322,9 +2381,10 @@ aifmm_status aifmm_kernel_profile_read(aifmm_problem* p, int kind, long* launche
 
 aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n) {
   if (!p || !out) return AIFMM_ERR_ARG;
-  const double v[8] = {p->st_sync_ms, (double)p->st_syncs, p->st_pending_ms, p->st_elim_ms, p->st_back_ms,
-                       (double)p->st_compress, p->ms[3], (double)p->launches_fs};
-  for (int i = 0; i < n && i < 8; ++i) out[i] = v[i];
+  const double v[12] = {p->st_sync_ms, (double)p->st_syncs, p->st_pending_ms, p->st_elim_ms, p->st_back_ms,
+                        (double)p->st_compress, p->ms[3], (double)p->launches_fs,
+                        p->st_asm_lists_ms, p->st_asm_aca_ms, p->st_asm_lu_ms, p->st_asm_blocks_ms};
+  for (int i = 0; i < n && i < 12; ++i) out[i] = v[i];
   return AIFMM_OK;
 }
 

@@ -142,7 +142,9 @@ aifmm_status aifmm_kernel_profile_read(aifmm_problem* p, int kind, long* launche
 /* Host-side statistics of the last factorize_solve: [0] ms waiting in stream syncs,
  * [1] number of syncs, [2] ms in pending-pair handling (recompression), [3] ms in the
  * per-box elimination, [4] ms in back substitution, [5] recompressions, [6] total ms,
- * [7] kernel launches. */
+ * [7] kernel launches; of the last assemble: [8] ms building index lists on the host,
+ * [9] ms in the ACA (launch to ranks on the host), [10] ms for the interpolative
+ * operators, [11] ms for the M2L and P2P block entries.  n <= 12 values are written. */
 aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n);
 /* The CUDA stream the handle works on (cudaStream_t). */
 aifmm_status aifmm_get_stream(const aifmm_problem* p, void** stream);
