@@ -273,10 +273,10 @@ class FMM2DTree:
         return ms
 
     def stats(self):
-        v = np.zeros(12)
-        self._ck(load().aifmm_stats(self.K.h, _dp(v), 12))
+        v = np.zeros(13)
+        self._ck(load().aifmm_stats(self.K.h, _dp(v), 13))
         keys = ["sync_ms", "syncs", "pending_ms", "elim_ms", "back_ms", "compressions", "total_ms", "launches",
-                "asm_lists_ms", "asm_aca_ms", "asm_lu_ms", "asm_blocks_ms"]
+                "asm_lists_ms", "asm_aca_ms", "asm_lu_ms", "asm_blocks_ms", "asm_aca_gpu_ms"]
         return dict(zip(keys, v.tolist()))
 
     def kernel_profile(self, kind, enable=True):

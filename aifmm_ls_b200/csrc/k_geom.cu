@@ -95,7 +95,26 @@ __global__ void rhs_kernel(const double2* __restrict__ pts, const double* __rest
   }
 }
 
+// dst[g.x, g.x + g.z) = src[g.y, g.y + g.z) for every segment g: one warp per segment
+__global__ void gather_segments_kernel(const int* __restrict__ src, const int4* __restrict__ segs, long nseg,
+                                       int* __restrict__ dst) {
+  const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  for (long w = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nseg; w += nwarps) {
+    const int4 g = segs[w];
+    for (int i = lane; i < g.z; i += 32) dst[(long)g.x + i] = src[(long)g.y + i];
+  }
+}
+
 }  // namespace
+
+int aifmm_launch_gather_segments(const int* src, const int4* segs, long nseg, int* dst, cudaStream_t s) {
+  if (nseg <= 0) return 0;
+  long blocks = (nseg * 32 + 255) / 256;
+  if (blocks > 148L * 32) blocks = 148L * 32;
+  gather_segments_kernel<<<(int)blocks, 256, 0, s>>>(src, segs, nseg, dst);
+  return (int)cudaGetLastError();
+}
 
 int aifmm_launch_geometry(int n_cheb, int depth, double L, int q_kind, double q_amp, double q_width, double q_radius,
                           const double* cheb, double2* pts, double* q, double2* leafc, int2* leafxy,

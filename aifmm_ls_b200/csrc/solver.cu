@@ -12,6 +12,7 @@
 // next: the ACA ranks of a level, the recompression ranks, and the norms that
 // decide which fill-ins are queued for recompression.
 #include <algorithm>
+#include <climits>
 #include <cfloat>
 #include <chrono>
 #include <cmath>
@@ -34,6 +35,7 @@ int aifmm_launch_geometry(int n_cheb, int depth, double L, int q_kind, double q_
                           cudaStream_t s);
 int aifmm_launch_rhs_plane_wave(const double2* pts, const double* q, double kappa, int N, int nrhs,
                                 const double* theta, double2* b, cudaStream_t s);
+int aifmm_launch_gather_segments(const int* src, const int4* segs, long nseg, int* dst, cudaStream_t s);
 
 namespace {
 
@@ -598,7 +600,7 @@ struct aifmm_problem {
   double st_sync_ms = 0, st_compress_ms = 0, st_elim_ms = 0, st_back_ms = 0, st_pending_ms = 0;
   // assembly split: host index lists, ACA (launch to ranks on the host),
   // interpolative operators, M2L/P2P block entries (launch to completion)
-  double st_asm_lists_ms = 0, st_asm_aca_ms = 0, st_asm_lu_ms = 0, st_asm_blocks_ms = 0;
+  double st_asm_lists_ms = 0, st_asm_aca_ms = 0, st_asm_lu_ms = 0, st_asm_blocks_ms = 0, st_asm_aca_gpu_ms = 0;
   long st_syncs = 0, st_compress = 0, st_apicalls = 0;
   void sync() {
     auto t0 = std::chrono::steady_clock::now();
@@ -783,34 +785,75 @@ struct aifmm_problem {
     const EntryCtx cx = ctx();
     using clk = std::chrono::steady_clock;
     auto since = [](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
-    st_asm_lists_ms = st_asm_aca_ms = st_asm_lu_ms = st_asm_blocks_ms = 0;
+    st_asm_lists_ms = st_asm_aca_ms = st_asm_lu_ms = st_asm_blocks_ms = st_asm_aca_gpu_ms = 0;
+    cudaEvent_t ea = nullptr, eb = nullptr;
+    CK(cudaEventCreate(&ea));
+    CK(cudaEventCreate(&eb));
     for (int j = depth; j >= 2; --j) {
       const int nbx = nBoxes[j];
       auto ta = clk::now();
-      // ---- index lists for the outgoing and incoming ACA of every box (F:1230-1336)
-      std::vector<int> idx;
+      // ---- index lists for the outgoing and incoming ACA of every box (F:1230-1336).
+      // The point lists of this level's boxes (rows_for) go to the device once; a
+      // job's row and column lists are concatenations of them, expanded on the
+      // device from a table of (destination, source, length) segments.
+      std::vector<int> lst;  // in-lists of all boxes, then out-lists
+      std::vector<long> lin_off(nbx + 1), lout_off(nbx + 1);
+      for (int k = 0; k < nbx; ++k) { lin_off[k] = (long)lst.size(); rows_for(j, k, true, lst); }
+      lin_off[nbx] = (long)lst.size();
+      for (int k = 0; k < nbx; ++k) { lout_off[k] = (long)lst.size(); rows_for(j, k, false, lst); }
+      lout_off[nbx] = (long)lst.size();
+      auto lin_len = [&](int b) { return (int)(lin_off[b + 1] - lin_off[b]); };
+      auto lout_len = [&](int b) { return (int)(lout_off[b + 1] - lout_off[b]); };
+      std::vector<int> ilb;  // interaction-list boxes of every box: inner, then outer (il_nodes order)
+      std::vector<int> ilb_off(nbx + 1);
+      for (int k = 0; k < nbx; ++k) {
+        ilb_off[k] = (int)ilb.size();
+        const Box& B = T[j][k];
+        for (int i = 0; i < 16; ++i) if (B.inner[i] != -1) ilb.push_back(B.inner[i]);
+        for (int i = 0; i < 24; ++i) if (B.outer[i] != -1) ilb.push_back(B.outer[i]);
+      }
+      ilb_off[nbx] = (int)ilb.size();
+      // point of position rel in the concatenated in-lists (or out-lists) of k's interaction list
+      auto il_point = [&](int k, bool in_lists, int rel) {
+        for (int q = ilb_off[k]; q < ilb_off[k + 1]; ++q) {
+          const int b = ilb[q], len = in_lists ? lin_len(b) : lout_len(b);
+          if (rel < len) return lst[(in_lists ? lin_off[b] : lout_off[b]) + rel];
+          rel -= len;
+        }
+        throw Fail(AIFMM_ERR_NUMERIC, "skeleton index outside the interaction list");
+      };
       struct JobIdx { long r0, c0; int n1, n2; };
       std::vector<JobIdx> ji(2 * nbx);
-      std::vector<std::vector<int>> boxA_out(nbx), IL_out(nbx), boxA_in(nbx), IL_in(nbx);
+      std::vector<int4> segs;
+      long cur_i = 0;
+      auto seg = [&](long src, int len) {
+        if (len > 0) segs.push_back(make_int4((int)cur_i, (int)src, len, 0));
+        cur_i += len;
+      };
       for (int k = 0; k < nbx; ++k) {
-        rows_for(j, k, false, boxA_out[k]);
-        il_nodes(j, k, true, IL_out[k]);
-        rows_for(j, k, true, boxA_in[k]);
-        il_nodes(j, k, false, IL_in[k]);
-        // outgoing: rows = IL targets, cols = box sources
-        ji[2 * k] = {(long)idx.size(), 0, (int)IL_out[k].size(), (int)boxA_out[k].size()};
-        idx.insert(idx.end(), IL_out[k].begin(), IL_out[k].end());
-        ji[2 * k].c0 = (long)idx.size();
-        idx.insert(idx.end(), boxA_out[k].begin(), boxA_out[k].end());
-        // incoming: rows = box targets, cols = IL sources
-        ji[2 * k + 1] = {(long)idx.size(), 0, (int)boxA_in[k].size(), (int)IL_in[k].size()};
-        idx.insert(idx.end(), boxA_in[k].begin(), boxA_in[k].end());
-        ji[2 * k + 1].c0 = (long)idx.size();
-        idx.insert(idx.end(), IL_in[k].begin(), IL_in[k].end());
+        // outgoing: rows = IL targets (their in-lists), cols = box sources (k's out-list)
+        JobIdx& o = ji[2 * k];
+        o.r0 = cur_i; o.n1 = 0;
+        for (int q = ilb_off[k]; q < ilb_off[k + 1]; ++q) { const int b = ilb[q]; o.n1 += lin_len(b); seg(lin_off[b], lin_len(b)); }
+        o.c0 = cur_i; o.n2 = lout_len(k); seg(lout_off[k], o.n2);
+        // incoming: rows = box targets (k's in-list), cols = IL sources (their out-lists)
+        JobIdx& in = ji[2 * k + 1];
+        in.r0 = cur_i; in.n1 = lin_len(k); seg(lin_off[k], in.n1);
+        in.c0 = cur_i; in.n2 = 0;
+        for (int q = ilb_off[k]; q < ilb_off[k + 1]; ++q) { const int b = ilb[q]; in.n2 += lout_len(b); seg(lout_off[b], lout_len(b)); }
       }
+      if (cur_i > INT_MAX || (long)lst.size() > INT_MAX) throw Fail(AIFMM_ERR_NOMEM, "ACA index lists too long");
       int* d_idx = nullptr;
-      CK(cudaMalloc(&d_idx, sizeof(int) * std::max<size_t>(1, idx.size())));
-      if (!idx.empty()) CK(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, st));
+      int* d_lst = nullptr;
+      int4* d_segs = nullptr;
+      CK(cudaMalloc(&d_idx, sizeof(int) * std::max<long>(1, cur_i)));
+      CK(cudaMalloc(&d_lst, sizeof(int) * std::max<size_t>(1, lst.size())));
+      CK(cudaMalloc(&d_segs, sizeof(int4) * std::max<size_t>(1, segs.size())));
+      if (!lst.empty()) CK(cudaMemcpyAsync(d_lst, lst.data(), sizeof(int) * lst.size(), cudaMemcpyHostToDevice, st));
+      if (!segs.empty()) {
+        CK(cudaMemcpyAsync(d_segs, segs.data(), sizeof(int4) * segs.size(), cudaMemcpyHostToDevice, st));
+        KL(aifmm_launch_gather_segments(d_lst, d_segs, (long)segs.size(), d_idx, st));
+      }
       // ---- workspaces
       size_t ws = 0, nres = 0;
       std::vector<size_t> wo(2 * nbx), ro(2 * nbx);
@@ -857,7 +900,9 @@ struct aifmm_problem {
       st_asm_lists_ms += since(ta);
       ta = clk::now();
       const AcaJob* dj = stage.put(jobs, st);
+      CK(cudaEventRecord(ea, st));
       KL(aifmm_launch_aca(dj, (int)jobs.size(), tol, cx, st));
+      CK(cudaEventRecord(eb, st));
       // ---- ranks and skeletons back to the host
       std::vector<int> hres(2 * (size_t)2 * nbx + nres + 1);
       CK(cudaMemcpyAsync(hres.data(), d_res, sizeof(int) * hres.size(), cudaMemcpyDeviceToHost, st));
@@ -872,9 +917,16 @@ struct aifmm_problem {
         pb[t].assign(hb + ro[t], hb + ro[t] + rk[t]);
         sb[t].assign(hb + ro[t] + rmax, hb + ro[t] + rmax + rk[t]);
       }
+      {
+        float ms_ = 0;
+        CK(cudaEventElapsedTime(&ms_, ea, eb));
+        st_asm_aca_gpu_ms += ms_;
+      }
       cudaFree(d_res);
       cudaFree(d_ws);
       cudaFree(d_idx);
+      cudaFree(d_lst);
+      cudaFree(d_segs);
       st_asm_aca_ms += since(ta);
       ta = clk::now();
       // ---- skeletons, rank equalisation (F:1105-1113) and L2P / P2M jobs
@@ -884,14 +936,14 @@ struct aifmm_problem {
       for (int k = 0; k < nbx; ++k) {
         Box& B = T[j][k];
         B.in_check.clear(); B.in_charge.clear(); B.out_check.clear(); B.out_charge.clear();
-        // outgoing (t = 2k): rows = IL_out, cols = boxA_out
+        // outgoing (t = 2k): rows = the IL boxes' in-lists, cols = k's out-list
         {
           const int t = 2 * k;
           const auto& rb = br[t] == 1 ? pb[t] : sb[t];
           const auto& cb = br[t] == 1 ? sb[t] : pb[t];
           B.rank_out = rk[t];
-          for (int r : rb) B.out_check.push_back(IL_out[k][r]);
-          for (int c : cb) B.out_charge.push_back(boxA_out[k][c]);
+          for (int r : rb) B.out_check.push_back(il_point(k, true, r));
+          for (int c : cb) B.out_charge.push_back(lst[lout_off[k] + c]);
           B.Ar.r = rk[t];
         }
         {
@@ -899,8 +951,8 @@ struct aifmm_problem {
           const auto& rb = br[t] == 1 ? pb[t] : sb[t];
           const auto& cb = br[t] == 1 ? sb[t] : pb[t];
           B.rank_in = rk[t];
-          for (int r : rb) B.in_check.push_back(boxA_in[k][r]);
-          for (int c : cb) B.in_charge.push_back(IL_in[k][c]);
+          for (int r : rb) B.in_check.push_back(lst[lin_off[k] + r]);
+          for (int c : cb) B.in_charge.push_back(il_point(k, false, c));
           B.Ac.c = rk[t];
         }
         const size_t r = std::min(B.in_check.size(), B.out_check.size());
@@ -921,7 +973,7 @@ struct aifmm_problem {
       for (int k = 0; k < nbx; ++k) {
         Box& B = T[j][k];
         const int r = (int)B.in_check.size();
-        const int m_in = (int)boxA_in[k].size(), m_out = (int)boxA_out[k].size();
+        const int m_in = lin_len(k), m_out = lout_len(k);
         drop(B.L2P); drop(B.P2M);
         B.L2P = newblk(m_in, r);
         B.P2M = newblk(r, m_out);
@@ -1007,6 +1059,8 @@ struct aifmm_problem {
       for (int k = 0; k < nBoxes[j]; ++k) { Box& B = T[j][k]; B.NumM = B.P2M.r; B.NumL = B.L2P.c; }
     sync();
     st_asm_blocks_ms = since(tb);
+    cudaEventDestroy(ea);
+    cudaEventDestroy(eb);
     pool.commit_frees();
     assembled = true;
     launches_asm = launches_ - l0;
@@ -2381,10 +2435,11 @@ aifmm_status aifmm_kernel_profile_read(aifmm_problem* p, int kind, long* launche
 
 aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n) {
   if (!p || !out) return AIFMM_ERR_ARG;
-  const double v[12] = {p->st_sync_ms, (double)p->st_syncs, p->st_pending_ms, p->st_elim_ms, p->st_back_ms,
+  const double v[13] = {p->st_sync_ms, (double)p->st_syncs, p->st_pending_ms, p->st_elim_ms, p->st_back_ms,
                         (double)p->st_compress, p->ms[3], (double)p->launches_fs,
-                        p->st_asm_lists_ms, p->st_asm_aca_ms, p->st_asm_lu_ms, p->st_asm_blocks_ms};
-  for (int i = 0; i < n && i < 12; ++i) out[i] = v[i];
+                        p->st_asm_lists_ms, p->st_asm_aca_ms, p->st_asm_lu_ms, p->st_asm_blocks_ms,
+                        p->st_asm_aca_gpu_ms};
+  for (int i = 0; i < n && i < 13; ++i) out[i] = v[i];
   return AIFMM_OK;
 }
 

@@ -144,7 +144,8 @@ aifmm_status aifmm_kernel_profile_read(aifmm_problem* p, int kind, long* launche
  * per-box elimination, [4] ms in back substitution, [5] recompressions, [6] total ms,
  * [7] kernel launches; of the last assemble: [8] ms building index lists on the host,
  * [9] ms in the ACA (launch to ranks on the host), [10] ms for the interpolative
- * operators, [11] ms for the M2L and P2P block entries.  n <= 12 values are written. */
+ * operators, [11] ms for the M2L and P2P block entries, [12] ms of ACA kernel time
+ * (CUDA events).  n <= 13 values are written. */
 aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n);
 /* The CUDA stream the handle works on (cudaStream_t). */
 aifmm_status aifmm_get_stream(const aifmm_problem* p, void** stream);
