@@ -1564,51 +1564,45 @@ struct aifmm_problem {
     equalise(nLb, nPtb);
     Box& K = T[j][k];
     Box& Bb = T[j][b];
-    // first half: k's locals and b's multipoles
-    assign(K.M2L[b], persist_copy(kb.M2L, nLk.c, nPtb.c));
+    // The two halves (k's locals with b's multipoles; b's locals with k's
+    // multipoles) touch disjoint blocks -- M2L[k][x] and M2L[x][b] against M2L[b][x]
+    // and M2L[x][k], and the distinct parents of two well-separated boxes -- so
+    // each stage of both halves is one batched launch.
+    // stage 1: the new M2L blocks, the transfer matrices, the new bases
+    Blk m2l_kb = persist_copy(kb.M2L, nLk.c, nPtb.c), m2l_bk = persist_copy(bk.M2L, nLb.c, nPtk.c);
     Blk Tk = scr(nLk.c, K.L2P.c), Tb = scr(Bb.P2M.r, nPtb.c);
+    Blk Tk2 = scr(nLb.c, Bb.L2P.c), Tb2 = scr(K.P2M.r, nPtk.c);
     gemm(Tk, nLk, 1, K.L2P, 0, C1, C0);
     gemm(Tb, Bb.P2M, 0, nPtb, 0, C1, C0);
+    gemm(Tk2, nLb, 1, Bb.L2P, 0, C1, C0);
+    gemm(Tb2, K.P2M, 0, nPtk, 0, C1, C0);
+    Blk Lk = persist_copy(nLk, nLk.r, nLk.c), Pmb = persist_adj(nPtb);
+    Blk Lb = persist_copy(nLb, nLb.r, nLb.c), Pmk = persist_adj(nPtk);
     flush_geam();
     flush_gemm();
+    // stage 2: the other M2L blocks of the four changed bases, and the parents
+    assign(K.M2L[b], m2l_kb);
     update_other_M2Ls_at_k(j, k, b, Tk);
     update_other_M2Ls_at_b(j, k, b, Tb);
     if (j > 2) { update_parent_L2P(j, k, Tk); update_parent_P2M(j, b, Tb); }
-    flush_geam();
-    flush_gemm();
-    {
-      Blk L = persist_copy(nLk, nLk.r, nLk.c);
-      Blk Pm = persist_adj(nPtb);
-      flush_geam();
-      assign(K.L2P, L);
-      assign(Bb.P2M, Pm);
-    }
+    assign(K.L2P, Lk);
+    assign(Bb.P2M, Pmb);
     K.NumL = K.L2P.c;
     Bb.NumM = Bb.P2M.r;
-    // second half: b's locals and k's multipoles
-    assign(Bb.M2L[k], persist_copy(bk.M2L, nLb.c, nPtk.c));
-    Blk Tk2 = scr(nLb.c, Bb.L2P.c), Tb2 = scr(K.P2M.r, nPtk.c);
-    gemm(Tk2, nLb, 1, Bb.L2P, 0, C1, C0);
-    gemm(Tb2, K.P2M, 0, nPtk, 0, C1, C0);
-    flush_geam();
-    flush_gemm();
+    assign(Bb.M2L[k], m2l_bk);
     update_other_M2Ls_at_k(j, b, k, Tk2);
     update_other_M2Ls_at_b(j, b, k, Tb2);
     if (j > 2) { update_parent_L2P(j, b, Tk2); update_parent_P2M(j, k, Tb2); }
-    flush_geam();
-    flush_gemm();
-    {
-      Blk L = persist_copy(nLb, nLb.r, nLb.c);
-      Blk Pm = persist_adj(nPtk);
-      flush_geam();
-      assign(Bb.L2P, L);
-      assign(K.P2M, Pm);
-    }
+    assign(Bb.L2P, Lb);
+    assign(K.P2M, Pmk);
     Bb.NumL = Bb.L2P.c;
     K.NumM = K.P2M.r;
+    flush_geam();
+    flush_gemm();
     // the Q blocks were fresh pool allocations; return them
     drop(kb.nL); drop(kb.nPt); drop(bk.nL); drop(bk.nPt);
   }
+
 
   void compress_M2P_P2L(int j, int k, int b) {  // F:1492-1530 (k not eliminated, b eliminated)
     ++st_compress;
@@ -1657,28 +1651,27 @@ struct aifmm_problem {
     geam(M2Lbk, Rnp, 1, C1, C1);
     flush_geam();
     equalise(nLk, nPtk);
-    assign(K.M2L[b], persist_copy(M2Lkb, nLk.c, M2Lkb.c));
-    Blk Tk = scr(nLk.c, K.L2P.c);
+    // k's locals and k's multipoles change; the updates touch M2L[k][x], M2L[x][k]
+    // and two different blocks of k's parent, so each stage is one batched launch
+    Blk m2l_kb = persist_copy(M2Lkb, nLk.c, M2Lkb.c), m2l_bk = persist_copy(M2Lbk, M2Lbk.r, nPtk.c);
+    Blk Tk = scr(nLk.c, K.L2P.c), Tb = scr(K.P2M.r, nPtk.c);
     gemm(Tk, nLk, 1, K.L2P, 0, C1, C0);
+    gemm(Tb, K.P2M, 0, nPtk, 0, C1, C0);
+    Blk L = persist_copy(nLk, nLk.r, nLk.c), Pm = persist_adj(nPtk);
     flush_geam();
     flush_gemm();
+    assign(K.M2L[b], m2l_kb);
     update_other_M2Ls_at_k(j, k, b, Tk);
     if (j > 2) update_parent_L2P(j, k, Tk);
-    flush_geam();
-    flush_gemm();
-    { Blk L = persist_copy(nLk, nLk.r, nLk.c); flush_geam(); assign(K.L2P, L); }
-    K.NumL = K.L2P.c;
-    assign(Bb.M2L[k], persist_copy(M2Lbk, M2Lbk.r, nPtk.c));
-    Blk Tb = scr(K.P2M.r, nPtk.c);
-    gemm(Tb, K.P2M, 0, nPtk, 0, C1, C0);
-    flush_geam();
-    flush_gemm();
+    assign(Bb.M2L[k], m2l_bk);
     update_other_M2Ls_at_b(j, b, k, Tb);
     if (j > 2) update_parent_P2M(j, k, Tb);
+    assign(K.L2P, L);
+    assign(K.P2M, Pm);
+    K.NumL = K.L2P.c;
+    K.NumM = K.P2M.r;
     flush_geam();
     flush_gemm();
-    { Blk Pm = persist_adj(nPtk); flush_geam(); assign(K.P2M, Pm); }
-    K.NumM = K.P2M.r;
     drop(nLk);
     drop(nPtk);
   }
