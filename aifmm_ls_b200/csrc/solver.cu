@@ -1177,6 +1177,11 @@ struct aifmm_problem {
         if (!T[j][nn].elim) assign(B.P2M_f[nn], t); else assign(B.M2M_f[nn], t);
       }
       { Blk t = newblk(B.P2M.r, nrhs); gemm(t, B.P2M, 0, Xb, 0, CM1, C0); assign(B.lrhs, t); }
+      // box k's own products first: the z-phase factorisation and solves need only
+      // them, and run on the second stream while the fill-ins of the neighbours'
+      // blocks below are computed
+      flush_gemm();
+      eliminate_z_side(j, k);
       for (int n = 0; n < 8; ++n) {
         const int nn = B.nb[n];
         if (nn == -1) continue;
@@ -1245,22 +1250,44 @@ struct aifmm_problem {
     }
   }
 
+  // The factorisation of L2M_f and its solves (F:2090-2113, 2245-2279): they read
+  // L2M_f, P2M_f / M2M_f and the local right-hand side of box k and write only k's
+  // own blocks, while the x-phase fill-ins write only the neighbours' blocks.
+  bool sz_on = false;
+  void eliminate_z_qr_solves(int j, int k) {
+    Box& B = T[j][k];
+    qr_prepare(B.qz, B.L2M_f, 0.0, true);
+    flush_qr();
+    const int nl = B.L2M_f.c;
+    { Blk t = newblk(nl, B.NumM); solve(B.qz, Blk(), t, CM1, true); assign(B.M2L[k], t); }  // QR2^{-1}(-I)
+    for (int n = 0; n < 8; ++n) {
+      const int nn = B.nb[n];
+      if (nn == -1) continue;
+      if (!T[j][nn].elim) { Blk t = newblk(nl, B.P2M_f[nn].c); solve(B.qz, B.P2M_f[nn], t, C1); assign(B.P2L[nn], t); }
+      else { Blk t = newblk(nl, B.M2M_f[nn].c); solve(B.qz, B.M2M_f[nn], t, C1); assign(B.M2L[nn], t); }
+      // well-separated test of (k, nn) is false for a neighbour: nothing is queued here
+    }
+    { Blk t = newblk(nl, nrhs); solve(B.qz, B.lrhs, t, C1); assign(B.mrhs, t); }
+    flush_solve();
+  }
+  void eliminate_z_side(int j, int k) {
+    sz_on = false;
+    if (T[j][k].L2M_f.size() == 0) return;
+    flush_all();
+    CK(cudaEventRecord(ev_fork, st));
+    CK(cudaStreamWaitEvent(st2, ev_fork, 0));
+    cur = st2;
+    eliminate_z_qr_solves(j, k);
+    CK(cudaEventRecord(ev_join, st2));
+    cur = st;
+    sz_on = true;
+  }
   void eliminate_z(int j, int k) {  // F:2090-2113, 2245-2372 (and the no-QR branch :2116-2242)
     Box& B = T[j][k];
     if (B.L2M_f.size() > 0) {
-      qr_prepare(B.qz, B.L2M_f, 0.0, true);
-      flush_qr();
-      const int nl = B.L2M_f.c;
-      { Blk t = newblk(nl, B.NumM); solve(B.qz, Blk(), t, CM1, true); assign(B.M2L[k], t); }  // QR2^{-1}(-I)
-      for (int n = 0; n < 8; ++n) {
-        const int nn = B.nb[n];
-        if (nn == -1) continue;
-        if (!T[j][nn].elim) { Blk t = newblk(nl, B.P2M_f[nn].c); solve(B.qz, B.P2M_f[nn], t, C1); assign(B.P2L[nn], t); }
-        else { Blk t = newblk(nl, B.M2M_f[nn].c); solve(B.qz, B.M2M_f[nn], t, C1); assign(B.M2L[nn], t); }
-        // well-separated test of (k, nn) is false for a neighbour: nothing is queued here
-      }
-      { Blk t = newblk(nl, nrhs); solve(B.qz, B.lrhs, t, C1); assign(B.mrhs, t); }
-      flush_solve();
+      if (sz_on) CK(cudaStreamWaitEvent(st, ev_join, 0));
+      else eliminate_z_qr_solves(j, k);
+      sz_on = false;
       const Blk Yneg = B.M2L[k], Yrhs = B.mrhs;
       for (int n = 0; n < 8; ++n) {
         const int nn = B.nb[n];
