@@ -65,6 +65,7 @@ SIGNATURES = {
     "aifmm_assemble": ([_v], ctypes.c_int),
     "aifmm_factorize_solve": ([_v, ctypes.c_int, _d, _d, ctypes.c_int], ctypes.c_int),
     "aifmm_dense_matvec": ([_v, ctypes.c_int, _d, _d, ctypes.c_int], ctypes.c_int),
+    "aifmm_total_field": ([_v, ctypes.c_int, _d, _d, _d, ctypes.c_int], ctypes.c_int),
     "aifmm_level_ranks": ([_v, ctypes.c_int, _i, _i], ctypes.c_int),
     "aifmm_box_skeleton": ([_v, ctypes.c_int, ctypes.c_int, ctypes.c_int, _i, ctypes.c_int, _i], ctypes.c_int),
     "aifmm_phase_times": ([_v, _d], ctypes.c_int),
@@ -208,6 +209,19 @@ class LSKernel:
         self._ck(load().aifmm_dense_matvec(self.h, x.shape[0], _dp(xi.view(np.float64)), _dp(y.view(np.float64)),
                                            PTR_HOST))
         return y
+
+    def total_field(self, theta, phi):
+        """u = u_inc + G phi (hybrid.cpp:263-281): the incident plane wave at each angle
+        plus the scattered field of the solution phi, with G the findPhi = false
+        operator (LS/LS_Assembly.hpp:474-541).  theta: (nrhs,), phi: (nrhs, N)."""
+        th = np.ascontiguousarray(np.atleast_1d(theta), dtype=np.float64)
+        phi = np.ascontiguousarray(np.atleast_2d(np.asarray(phi, dtype=np.complex128)))
+        if phi.shape[0] != th.size:
+            raise ValueError("one angle per right-hand side")
+        u = np.zeros_like(phi)
+        self._ck(load().aifmm_total_field(self.h, th.size, _dp(th), _dp(phi.view(np.float64)),
+                                          _dp(u.view(np.float64)), PTR_HOST))
+        return u
 
 
 class FMM2DTree:

@@ -108,6 +108,11 @@ __device__ __forceinline__ int near_dir(int dx, int dy) {
   return tab[(dy + 1) * 3 + (dx + 1)];
 }
 
+// PHI = true: the system matrix A (findPhi, LS_Assembly.hpp:506-511, 528-533);
+// PHI = false: the bare integral operator G of the same entry (no kappa^2 q(x_i)
+// factor, no identity), the operator the reference applies to the solution to
+// get the scattered field (hybrid.cpp:263-281).
+template <bool PHI = true>
 __device__ __forceinline__ double2 lsa_entry(int i, int j, const EntryCtx& c) {
   const int rank = c.rank;
   const int li = i / rank, ii = i - li * rank;
@@ -119,11 +124,13 @@ __device__ __forceinline__ double2 lsa_entry(int i, int j, const EntryCtx& c) {
   if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1) {
     const int dir = near_dir(dx, dy);
     double2 e = __ldg(&c.nearT[(size_t)dir * rank * rank + ii + (size_t)jj * rank]);
-    // entry*kappa*kappa*q evaluated left to right (LS_Assembly.hpp:508)
-    e.x = e.x * c.kappa; e.y = e.y * c.kappa;
-    e.x = e.x * c.kappa; e.y = e.y * c.kappa;
-    e.x = e.x * qi; e.y = e.y * qi;
-    if (i == j) e.x = 1.0 + e.x;
+    if (PHI) {
+      // entry*kappa*kappa*q evaluated left to right (LS_Assembly.hpp:508)
+      e.x = e.x * c.kappa; e.y = e.y * c.kappa;
+      e.x = e.x * c.kappa; e.y = e.y * c.kappa;
+      e.x = e.x * qi; e.y = e.y * qi;
+      if (i == j) e.x = 1.0 + e.x;
+    }
     if (hypot(e.x, e.y) < 1e-16) e = make_double2(0.0, 0.0);
     return e;
   }
@@ -135,9 +142,11 @@ __device__ __forceinline__ double2 lsa_entry(int i, int j, const EntryCtx& c) {
   double2 s = far_series(R, th, c.M + (size_t)jj * (2 * AIFMM_SERIES + 1));
   // *= I/4 (exact), then *= kappa*kappa*q (LS_Assembly.hpp:529-531)
   s = make_double2(-0.25 * s.y, 0.25 * s.x);
-  const double kq = c.kappa * c.kappa * qi;
-  s.x *= kq; s.y *= kq;
-  if (i == j) s.x += 1.0;
+  if (PHI) {
+    const double kq = c.kappa * c.kappa * qi;
+    s.x *= kq; s.y *= kq;
+    if (i == j) s.x += 1.0;
+  }
   if (hypot(s.x, s.y) < 1e-16) s = make_double2(0.0, 0.0);
   return s;
 }

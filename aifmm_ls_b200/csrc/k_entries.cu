@@ -40,6 +40,7 @@ __global__ void list_entries_kernel(const int* __restrict__ I, const int* __rest
 // combined with atomics.
 constexpr int kMvRows = 128;
 constexpr int kMvMaxRhs = 8;
+template <bool PHI>
 __global__ void __launch_bounds__(kMvRows) dense_matvec_kernel(const double2* __restrict__ x, double2* y, int N,
                                                                 int nrhs, int cols_per_slice, EntryCtx ctx) {
   const int i = blockIdx.x * kMvRows + threadIdx.x;
@@ -49,7 +50,7 @@ __global__ void __launch_bounds__(kMvRows) dense_matvec_kernel(const double2* __
   double2 acc[kMvMaxRhs];
   for (int s = 0; s < kMvMaxRhs; ++s) acc[s] = make_double2(0.0, 0.0);
   for (int j = j0; j < j1; ++j) {
-    double2 a = lsa_entry(i, j, ctx);
+    double2 a = lsa_entry<PHI>(i, j, ctx);
     if (a.x == 0.0 && a.y == 0.0) continue;
     for (int s = 0; s < nrhs; ++s) acc[s] = cfma(a, __ldg(&x[j + (size_t)s * N]), acc[s]);
   }
@@ -79,10 +80,10 @@ int aifmm_launch_list_entries(const int* I, const int* J, long n, double2* out, 
   return (int)cudaGetLastError();
 }
 
-int aifmm_launch_dense_matvec(const double2* x, double2* y, int N, int nrhs, const EntryCtx& ctx,
-                              cudaStream_t stream) {
+namespace {
+template <bool PHI>
+int launch_matvec(const double2* x, double2* y, int N, int nrhs, const EntryCtx& ctx, cudaStream_t stream) {
   if (nrhs > kMvMaxRhs) return (int)cudaErrorInvalidValue;
-  cudaMemsetAsync(y, 0, sizeof(double2) * (size_t)N * nrhs, stream);
   const int row_blocks = (N + kMvRows - 1) / kMvRows;
   // enough slices to give every SM several CTAs
   int slices = (148 * 8 + row_blocks - 1) / row_blocks;
@@ -90,6 +91,18 @@ int aifmm_launch_dense_matvec(const double2* x, double2* y, int N, int nrhs, con
   int cps = (N + slices - 1) / slices;
   slices = (N + cps - 1) / cps;
   dim3 grid(row_blocks, slices);
-  dense_matvec_kernel<<<grid, kMvRows, 0, stream>>>(x, y, N, nrhs, cps, ctx);
+  dense_matvec_kernel<PHI><<<grid, kMvRows, 0, stream>>>(x, y, N, nrhs, cps, ctx);
   return (int)cudaGetLastError();
+}
+}  // namespace
+
+int aifmm_launch_dense_matvec(const double2* x, double2* y, int N, int nrhs, const EntryCtx& ctx,
+                              cudaStream_t stream) {
+  if (nrhs > kMvMaxRhs) return (int)cudaErrorInvalidValue;
+  cudaMemsetAsync(y, 0, sizeof(double2) * (size_t)N * nrhs, stream);
+  return launch_matvec<true>(x, y, N, nrhs, ctx, stream);
+}
+int aifmm_launch_green_matvec_add(const double2* x, double2* y, int N, int nrhs, const EntryCtx& ctx,
+                                  cudaStream_t stream) {
+  return launch_matvec<false>(x, y, N, nrhs, ctx, stream);
 }

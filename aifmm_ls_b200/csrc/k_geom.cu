@@ -95,6 +95,22 @@ __global__ void rhs_kernel(const double2* __restrict__ pts, const double* __rest
   }
 }
 
+// u_inc = exp(i kappa (x cos t + y sin t)) at every grid point (LS/LS_functions.hpp:113-116
+// is the t = 0 case)
+__global__ void incident_kernel(const double2* __restrict__ pts, double kappa, int N, int nrhs,
+                                const double* __restrict__ theta, double2* u) {
+  const long tot = (long)N * nrhs;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % N), s = (int)(t / N);
+    double ct = cos(theta[s]), st = sin(theta[s]);
+    if (theta[s] == 0.0) { ct = 1.0; st = 0.0; }
+    const double ph = pts[i].x * ct + pts[i].y * st;
+    double sn, cs;
+    sincos(kappa * ph, &sn, &cs);
+    u[t] = make_double2(cs, sn);
+  }
+}
+
 // dst[g.x, g.x + g.z) = src[g.y, g.y + g.z) for every segment g: one warp per segment
 __global__ void gather_segments_kernel(const int* __restrict__ src, const int4* __restrict__ segs, long nseg,
                                        int* __restrict__ dst) {
@@ -107,6 +123,16 @@ __global__ void gather_segments_kernel(const int* __restrict__ src, const int4* 
 }
 
 }  // namespace
+
+int aifmm_launch_incident_field(const double2* pts, double kappa, int N, int nrhs, const double* theta, double2* u,
+                                cudaStream_t s) {
+  const long tot = (long)N * nrhs;
+  long blocks = (tot + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) return 0;
+  incident_kernel<<<(int)blocks, 256, 0, s>>>(pts, kappa, N, nrhs, theta, u);
+  return (int)cudaGetLastError();
+}
 
 int aifmm_launch_gather_segments(const int* src, const int4* segs, long nseg, int* dst, cudaStream_t s) {
   if (nseg <= 0) return 0;

@@ -124,6 +124,9 @@ int aifmm_launch_list_entries(const int* I, const int* J, long n, double2* out, 
                               cudaStream_t stream);
 int aifmm_launch_dense_matvec(const double2* x, double2* y, int N, int nrhs, const EntryCtx& ctx,
                               cudaStream_t stream);
+// y += G x with G the entries without kappa^2 q and identity (findPhi = false)
+int aifmm_launch_green_matvec_add(const double2* x, double2* y, int N, int nrhs, const EntryCtx& ctx,
+                                  cudaStream_t stream);
 int aifmm_launch_aca(const AcaJob* d_jobs, int njobs, double tol, const EntryCtx& ctx, cudaStream_t stream);
 int aifmm_launch_qr_factor(const QRJob* d_jobs, int njobs, cudaStream_t s);
 int aifmm_launch_qr_solve(const SolveJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s);

@@ -35,6 +35,8 @@ int aifmm_launch_geometry(int n_cheb, int depth, double L, int q_kind, double q_
                           cudaStream_t s);
 int aifmm_launch_rhs_plane_wave(const double2* pts, const double* q, double kappa, int N, int nrhs,
                                 const double* theta, double2* b, cudaStream_t s);
+int aifmm_launch_incident_field(const double2* pts, double kappa, int N, int nrhs, const double* theta, double2* u,
+                                cudaStream_t s);
 int aifmm_launch_gather_segments(const int* src, const int4* segs, long nseg, int* dst, cudaStream_t s);
 
 namespace {
@@ -2398,6 +2400,35 @@ aifmm_status aifmm_dense_matvec(aifmm_problem* p, int nrhs, const double* x, dou
       CK(cudaMemcpyAsync(y, ty, bytes, cudaMemcpyDeviceToHost, p->st));
       p->sync();
       cudaFree(tx); cudaFree(ty);
+    } else {
+      p->sync();
+    }
+  });
+}
+
+aifmm_status aifmm_total_field(aifmm_problem* p, int nrhs, const double* theta, const double* phi, double* u,
+                               int flags) {
+  if (!p || !theta || !phi || !u || nrhs < 1 || nrhs > 8) return AIFMM_ERR_ARG;
+  if (!p->tables_ready) { p->err = "tables not ready"; return AIFMM_ERR_STATE; }
+  return guard(p, [&] {
+    const size_t bytes = sizeof(double2) * (size_t)p->N * nrhs;
+    const bool dev = flags & AIFMM_PTR_DEVICE;
+    const double2* dphi = reinterpret_cast<const double2*>(phi);
+    double2* du = reinterpret_cast<double2*>(u);
+    double2 *tphi = nullptr, *tu = nullptr;
+    if (!dev) {
+      CK(cudaMalloc(&tphi, bytes)); CK(cudaMalloc(&tu, bytes));
+      CK(cudaMemcpyAsync(tphi, phi, bytes, cudaMemcpyHostToDevice, p->st));
+      dphi = tphi; du = tu;
+    }
+    const double* dth = static_cast<const double*>(p->stage.put_raw(theta, sizeof(double) * nrhs, p->st));
+    int e = aifmm_launch_incident_field(p->d_pts, p->d.kappa, p->N, nrhs, dth, du, p->st);
+    if (!e) e = aifmm_launch_green_matvec_add(dphi, du, p->N, nrhs, p->ctx(), p->st);
+    if (e) throw Fail(AIFMM_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
+    if (!dev) {
+      CK(cudaMemcpyAsync(u, tu, bytes, cudaMemcpyDeviceToHost, p->st));
+      p->sync();
+      cudaFree(tphi); cudaFree(tu);
     } else {
       p->sync();
     }

@@ -125,6 +125,16 @@ aifmm_status aifmm_factorize_solve(aifmm_problem* p, int nrhs, const double* b, 
  * y = A x with exact entries, x and y N x nrhs complex (nrhs <= 8). */
 aifmm_status aifmm_dense_matvec(aifmm_problem* p, int nrhs, const double* x, double* y, int flags);
 
+/* The total field from a solution (hybrid.cpp:263-281, with the kernel's findPhi
+ * switch of LS/LS_Assembly.hpp:474-541 off): u = u_inc + G phi, where
+ * u_inc = exp(i kappa (x cos t_s + y sin t_s)) for angle theta[s] (the reference's
+ * IncidenceFunction, LS/LS_functions.hpp:113-116, is t = 0) and G is the operator
+ * whose entries are the system entries without the kappa^2 q(x_i) factor and the
+ * identity.  Dense with exact entries; theta is a host array of nrhs angles; phi
+ * and u are N x nrhs complex (nrhs <= 8). */
+aifmm_status aifmm_total_field(aifmm_problem* p, int nrhs, const double* theta, const double* phi, double* u,
+                               int flags);
+
 /* Introspection: ranks of the ACA skeletons of a level after assemble (incoming, outgoing,
  * before the rank equalisation of get_L2P_P2M_box) and the skeleton point lists
  * (which: 0 incoming check, 1 incoming charge, 2 outgoing check, 3 outgoing charge). */

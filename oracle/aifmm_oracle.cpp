@@ -760,8 +760,9 @@ struct Problem {
     }
     return e;
   }
-  // LSA:474-541
-  cd entry0(int i, int j) const {
+  // LSA:474-541.  phi = the kernel's findPhi switch: true for the system matrix,
+  // false for the bare operator G used for the scattered field (LSA:506-511, 528-533)
+  cd entry0(int i, int j, bool phi = true) const {
     const int li = i / rank, ii = i % rank, lj = j / rank, jj = j % rank;
     int xi, yi, xj, yj;
     box_xy(li, depth, xi, yi);
@@ -773,8 +774,10 @@ struct Problem {
       for (int d = 0; d < 8; ++d)
         if (NB_DX[d] == dx && NB_DY[d] == dy) dir = d;
       cd e = T.near[(size_t)dir * rank * rank + ii + (size_t)jj * rank];
-      e = e * p.kappa * p.kappa * q[i];  // LSA:508, evaluated left to right
-      if (i == j) e = 1.0 + e;
+      if (phi) {
+        e = e * p.kappa * p.kappa * q[i];  // LSA:508, evaluated left to right
+        if (i == j) e = 1.0 + e;
+      }
       if (std::abs(e) < 1e-16) e = 0.0;
       return e;
     }
@@ -796,8 +799,10 @@ struct Problem {
       s += Mc[n + 60] * t;
     }
     s *= I1 / 4.0;
-    s *= p.kappa * p.kappa * q[i];  // LSA:531
-    if (i == j) s += 1.0;
+    if (phi) {
+      s *= p.kappa * p.kappa * q[i];  // LSA:531
+      if (i == j) s += 1.0;
+    }
     if (std::abs(s) < 1e-16) s = 0.0;
     return s;
   }
@@ -1824,6 +1829,32 @@ int orc_dense_matvec(void* h, int nrhs, const double* x, double* y) {
       for (int s = 0; s < nrhs; ++s) acc[s] += a * cd(x[2 * ((size_t)s * N + j)], x[2 * ((size_t)s * N + j) + 1]);
     }
     for (int s = 0; s < nrhs; ++s) { y[2 * ((size_t)s * N + i)] = acc[s].real(); y[2 * ((size_t)s * N + i) + 1] = acc[s].imag(); }
+  }
+  return 0;
+}
+
+// hybrid.cpp:263-281: U_total = U_incidence + G Phi with G the findPhi = false
+// operator, dense with exact entries; the incidence direction is (cos t, sin t)
+int orc_total_field(void* h, int nrhs, const double* theta, const double* phi, double* u) {
+  Problem* P = static_cast<Problem*>(h);
+  const int N = P->N;
+  const double k = P->p.kappa;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int i = 0; i < N; ++i) {
+    std::vector<cd> acc(nrhs, cd(0, 0));
+    for (int j = 0; j < N; ++j) {
+      cd g = P->entry0(i, j, false);
+      if (g == cd(0, 0)) continue;
+      for (int s = 0; s < nrhs; ++s) acc[s] += g * cd(phi[2 * ((size_t)s * N + j)], phi[2 * ((size_t)s * N + j) + 1]);
+    }
+    for (int s = 0; s < nrhs; ++s) {
+      double ct = std::cos(theta[s]), st = std::sin(theta[s]);
+      if (theta[s] == 0.0) { ct = 1.0; st = 0.0; }
+      const cd inc = std::exp(I1 * k * (P->pts[i].x * ct + P->pts[i].y * st));  // LS/LS_functions.hpp:113-116
+      const cd v = inc + acc[s];
+      u[2 * ((size_t)s * N + i)] = v.real();
+      u[2 * ((size_t)s * N + i) + 1] = v.imag();
+    }
   }
   return 0;
 }

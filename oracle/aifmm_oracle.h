@@ -66,6 +66,8 @@ int orc_rhs_plane_wave(void* h, int nrhs, const double* theta, double* b);
 int orc_entries(void* h, long n, const int* I, const int* J, double* out);
 /* y = A x for nrhs right-hand sides (dense, exact entries) */
 int orc_dense_matvec(void* h, int nrhs, const double* x, double* y);
+/* u = u_inc + G phi (the total field of hybrid.cpp:263-281; G = entries with findPhi off) */
+int orc_total_field(void* h, int nrhs, const double* theta, const double* phi, double* u);
 /* Full pipeline: assemble, eliminate_phase_efficient (with the rhs carried),
  * base solve, back substitution.  times[4] = tree, assemble, factor, solve (s). */
 int orc_solve(void* h, int nrhs, const double* b, double* x, double* times);

@@ -54,6 +54,7 @@ def lib():
         _lib.orc_rhs_plane_wave.argtypes = [v, ctypes.c_int, d, d]
         _lib.orc_entries.argtypes = [v, ctypes.c_long, i, i, d]
         _lib.orc_dense_matvec.argtypes = [v, ctypes.c_int, d, d]
+        _lib.orc_total_field.argtypes = [v, ctypes.c_int, d, d, d]
         _lib.orc_solve.argtypes = [v, ctypes.c_int, d, d, d]
         _lib.orc_set_variant.argtypes = [v, ctypes.c_int]
         _lib.orc_set_perturbation.argtypes = [v, ctypes.c_double]
@@ -177,6 +178,15 @@ class Problem:
         y = np.zeros_like(xi)
         lib().orc_dense_matvec(self.h, x.shape[0], _dp(xi), _dp(y))
         return y[..., 0] + 1j * y[..., 1]
+
+    def total_field(self, thetas, phi):
+        """u = u_inc + G phi (hybrid.cpp:263-281), phi: (nrhs, N) complex."""
+        th = np.ascontiguousarray(np.atleast_1d(thetas), dtype=np.float64)
+        phi = np.atleast_2d(phi)
+        pi = np.ascontiguousarray(np.stack([phi.real, phi.imag], -1))
+        u = np.zeros_like(pi)
+        lib().orc_total_field(self.h, len(th), _dp(th), _dp(pi), _dp(u))
+        return u[..., 0] + 1j * u[..., 1]
 
     def solve(self, b):
         """b: (nrhs, N) complex.  Returns x (nrhs, N) and phase times."""

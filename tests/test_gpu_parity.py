@@ -176,3 +176,25 @@ def test_dense_matvec_matches_oracle(oracle_mod, table_cache):
     y = K.dense_matvec(x)
     yo = P.dense_matvec(x)
     assert np.linalg.norm(y - yo) / np.linalg.norm(yo) <= 1e-12
+
+
+def test_total_field_matches_oracle(oracle_mod, table_cache):
+    """u = u_inc + G phi (the scattered-field post-processing of hybrid.cpp:263-281)
+    for the solver's own solution, against the oracle's dense product."""
+    import aifmm_ls_b200 as A
+    p, tabs = table_cache(depth=3, q_kind="gauss_aw", kappa=20.0)
+    K = _kernel(p, tabs)
+    T = A.FMM2DTree(K)
+    th = np.array([0.0, 0.9])
+    b = K.rhs_plane_wave(th)
+    T.createTree()
+    T.assemble()
+    phi = T.solve(b)
+    u = K.total_field(th, phi)
+    P = oracle_mod.Problem(p, *tabs[:2])
+    uo = P.total_field(th, phi)
+    assert np.linalg.norm(u - uo) / np.linalg.norm(uo) <= ENTRY_TOL
+    # kappa^2 q u + phi is the solver's residual A phi - b: about 2e-4 relative at
+    # this compression tolerance (the oracle's own solution gives the same)
+    q = P.contrast()
+    assert np.linalg.norm(p.kappa ** 2 * q * u + phi) / np.linalg.norm(phi) <= 1e-3

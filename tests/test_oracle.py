@@ -131,6 +131,26 @@ def test_oracle_depth2_is_exact(oracle_mod, table_cache):
 
 
 @pytest.mark.parametrize("q_kind", ["gauss_aw", "disk"])
+def test_total_field_satisfies_the_integral_equation(oracle_mod, table_cache, q_kind):
+    """A = I + kappa^2 diag(q) G with G the findPhi = false operator, and
+    b = -kappa^2 q u_inc, so the exact solution phi of A phi = b gives
+    kappa^2 q (u_inc + G phi) = -phi: the total field of hybrid.cpp:263-281 is
+    consistent with the system matrix.  (Entries below 1e-16 are zeroed in A and
+    in G separately, which is far below the tolerance.)"""
+    p, (M, near, _) = table_cache(depth=2, tol_pow=8, kappa=10.0)
+    p.q_kind = oracle_mod.Q_KINDS[q_kind]
+    P = oracle_mod.Problem(p, M, near)
+    th = [0.0, 1.3]
+    b = P.rhs_plane_wave(th)
+    phi = np.linalg.solve(P.dense(), b.T).T
+    u = P.total_field(th, phi)
+    q = P.contrast()
+    k2 = p.kappa ** 2
+    assert np.linalg.norm(k2 * q * u + phi) / np.linalg.norm(phi) < 1e-10
+    assert np.all(np.isfinite(u))
+
+
+@pytest.mark.parametrize("q_kind", ["gauss_aw", "disk"])
 def test_oracle_elimination_solves_compressed_matrix(oracle_mod, table_cache, q_kind):
     """With every fill-in recompressed (eliminate_phase) the elimination solves the
     compressed matrix to the recompression tolerance; the driver's variant
