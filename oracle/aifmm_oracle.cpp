@@ -34,6 +34,7 @@
 #include <map>
 #include <set>
 #include <utility>
+#include <memory>
 #include <vector>
 #include <omp.h>
 
@@ -690,6 +691,16 @@ struct Problem {
   int nrhs = 1;
   double perturb = 0.0;        // relative entry perturbation (sensitivity studies only)
   bool full_compress = false;  // eliminate_phase (F:2374) instead of the driver's _efficient
+  // Reorderings that the GPU solver uses, restated here so that tests can show
+  // they change no bit of the result (test-only; 0 = the reference's order):
+  //   1: back substitution in waves of mutually non-adjacent boxes;
+  //   2: the factorisation of P2P[k][k] and its solves with the right-hand side
+  //      and the neighbour blocks before the recompressions of step k;
+  //   4: the factorisation of L2M_f and its solves before the x-phase fill-ins.
+  int schedule = 0;
+  long ncompress = 0;
+  struct XEarly { bool on = false; std::unique_ptr<ColPivQR> qr; Mat Xb; Mat S[8]; } xe;
+  struct ZEarly { bool on = false; Mat Yneg, Yrhs, Z[8]; } ze;
 
   static void box_xy(int k, int level, int& ix, int& iy) {
     ix = iy = 0;
@@ -1208,20 +1219,40 @@ struct Problem {
   // The reference leaves several blocks uninitialised in the no-QR branches
   // (Eigen Mat(r,c)); the value those statements stand for is a product with
   // an empty inner dimension, i.e. zero, which is what is stored here.
+  // schedule bit 2: what eliminate_x computes from P2P[k][k], the right-hand side
+  // and the neighbour blocks alone, computed before the step's recompressions
+  void x_early(int j, int k) {
+    xe.on = false;
+    Box& B = tree[j][k];
+    if (B.P2P[k].size() == 0) return;
+    xe.qr.reset(new ColPivQR(B.P2P[k]));
+    xe.Xb = xe.qr->solve(B.particle_rhs);
+    for (int n = 0; n < 8; ++n) {
+      int nn = B.neighbors[n];
+      if (nn == -1) continue;
+      xe.S[n] = tree[j][nn].Eliminated ? xe.qr->solve(B.M2P[nn]) : xe.qr->solve(B.P2P[nn]);
+    }
+    xe.on = true;
+  }
   void eliminate_x(int j, int k) {
     Box& B = tree[j][k];
     if (B.P2P[k].size() != 0) {
-      ColPivQR QR(B.P2P[k]);
+      std::unique_ptr<ColPivQR> own;
+      if (!xe.on) own.reset(new ColPivQR(B.P2P[k]));
+      const ColPivQR& QR = xe.on ? *xe.qr : *own;
+      // QR^{-1} of the right-hand side and of X[k][nn] for neighbour n
+      auto solve_rhs = [&]() { return xe.on ? xe.Xb : QR.solve(B.particle_rhs); };
+      auto solve_nb = [&](int n, const Mat& src) { return xe.on ? xe.S[n] : QR.solve(src); };
       // F:1961-1987
       B.L2M_f = neg(mul(B.P2M, QR.solve(B.L2P)));
       for (int n = 0; n < 8; ++n) {
         int nn = B.neighbors[n];
         if (nn == -1) continue;
-        if (!tree[j][nn].Eliminated) B.P2M_f[nn] = neg(mul(B.P2M, QR.solve(B.P2P[nn])));
-        else B.M2M_f[nn] = neg(mul(B.P2M, QR.solve(B.M2P[nn])));
+        if (!tree[j][nn].Eliminated) B.P2M_f[nn] = neg(mul(B.P2M, solve_nb(n, B.P2P[nn])));
+        else B.M2M_f[nn] = neg(mul(B.P2M, solve_nb(n, B.M2P[nn])));
       }
-      B.local_rhs = neg(mul(B.P2M, QR.solve(B.particle_rhs)));
-      Mat Xb = QR.solve(B.particle_rhs);
+      B.local_rhs = neg(mul(B.P2M, solve_rhs()));
+      Mat Xb = solve_rhs();
       Mat XL = QR.solve(B.L2P);
       // QR^{-1} X[k][pp] for every neighbour pp (the reference re-solves these
       // for every equation nn; the value is the same)
@@ -1229,8 +1260,10 @@ struct Problem {
       for (int pI = 0; pI < 8; ++pI) {
         int pp = B.neighbors[pI];
         if (pp == -1) continue;
-        W[pI] = tree[j][pp].Eliminated ? QR.solve(B.M2P[pp]) : QR.solve(B.P2P[pp]);
+        W[pI] = solve_nb(pI, tree[j][pp].Eliminated ? B.M2P[pp] : B.P2P[pp]);
       }
+      xe.on = false;
+      if (schedule & 4) z_early(j, k);
       for (int n = 0; n < 8; ++n) {
         int nn = B.neighbors[n];
         if (nn == -1) continue;
@@ -1309,33 +1342,53 @@ struct Problem {
     }
   }
 
+  // The factorisation of L2M_f and its solves (F:2251-2279): they read only box
+  // k's own blocks and write only box k's own blocks.
+  void z_solves(int j, int k, Mat& Yneg, Mat& Yrhs, Mat* Z) {
+    Box& B = tree[j][k];
+    ColPivQR QR2(B.L2M_f);
+    const int r = B.NumMultipoles;
+    // F:2255-2279
+    B.M2L[k] = QR2.solve(neg(identity(r)));
+    for (int n = 0; n < 8; ++n) {
+      int nn = B.neighbors[n];
+      if (nn == -1) continue;
+      if (!tree[j][nn].Eliminated) {
+        B.P2L[nn] = QR2.solve(B.P2M_f[nn]);
+        if (is_well_separated(j, k, nn) && fnorm(B.P2L[nn]) > 1e-10) P2L_M2Pq.push_back({k, nn});
+      } else {
+        B.M2L[nn] = QR2.solve(B.M2M_f[nn]);
+      }
+    }
+    // F:2251-2253
+    B.multipole_rhs = QR2.solve(B.local_rhs);
+    Yneg = QR2.solve(neg(identity(r)));
+    Yrhs = QR2.solve(B.local_rhs);
+    for (int pI = 0; pI < 8; ++pI) {
+      int pp = B.neighbors[pI];
+      if (pp == -1) continue;
+      Z[pI] = tree[j][pp].Eliminated ? QR2.solve(B.M2M_f[pp]) : QR2.solve(B.P2M_f[pp]);
+    }
+  }
+  // schedule bit 4: z_solves before the x-phase fill-ins of the neighbours' blocks
+  void z_early(int j, int k) {
+    ze.on = false;
+    if (tree[j][k].L2M_f.size() == 0) return;
+    z_solves(j, k, ze.Yneg, ze.Yrhs, ze.Z);
+    ze.on = true;
+  }
   void eliminate_z(int j, int k) {
     Box& B = tree[j][k];
     if (B.L2M_f.size() > 0) {
-      ColPivQR QR2(B.L2M_f);
-      const int r = B.NumMultipoles;
-      // F:2255-2279
-      B.M2L[k] = QR2.solve(neg(identity(r)));
-      for (int n = 0; n < 8; ++n) {
-        int nn = B.neighbors[n];
-        if (nn == -1) continue;
-        if (!tree[j][nn].Eliminated) {
-          B.P2L[nn] = QR2.solve(B.P2M_f[nn]);
-          if (is_well_separated(j, k, nn) && fnorm(B.P2L[nn]) > 1e-10) P2L_M2Pq.push_back({k, nn});
-        } else {
-          B.M2L[nn] = QR2.solve(B.M2M_f[nn]);
-        }
+      Mat Yneg, Yrhs, Z[8];
+      if (ze.on) {
+        Yneg = ze.Yneg;
+        Yrhs = ze.Yrhs;
+        for (int q = 0; q < 8; ++q) Z[q] = ze.Z[q];
+      } else {
+        z_solves(j, k, Yneg, Yrhs, Z);
       }
-      // F:2251-2253
-      B.multipole_rhs = QR2.solve(B.local_rhs);
-      Mat Yneg = QR2.solve(neg(identity(r)));
-      Mat Yrhs = QR2.solve(B.local_rhs);
-      Mat Z[8];
-      for (int pI = 0; pI < 8; ++pI) {
-        int pp = B.neighbors[pI];
-        if (pp == -1) continue;
-        Z[pI] = tree[j][pp].Eliminated ? QR2.solve(B.M2M_f[pp]) : QR2.solve(B.P2M_f[pp]);
-      }
+      ze.on = false;
       for (int n = 0; n < 8; ++n) {
         int nn = B.neighbors[n];
         if (nn == -1) continue;
@@ -1584,15 +1637,18 @@ struct Problem {
   }
 
   void eliminate_phase_efficient() {  // F:2407-2451
+    ncompress = 0;
     for (int j = depth; j >= 2; --j) {
       if (j != depth) initialise_P2P_NonLeafLevel(j);
       for (int k = 0; k < nBoxes[j]; ++k) {
+        if (schedule & 2) x_early(j, k);
         for (size_t i = 0; i < P2Pq.size(); ++i) {
           int nn = P2Pq[i].first, pp = P2Pq[i].second;
           if (k == nn || k == pp) {
             P2Pq.erase(P2Pq.begin() + i);
             --i;
             if (tree[j][nn].P2P[pp].size() != 0) {
+              ++ncompress;
               compress_P2P_Two_Ways(j, nn, pp);
               tree[j][nn].P2P[pp] = Mat();
               tree[j][pp].P2P[nn] = Mat();
@@ -1605,6 +1661,7 @@ struct Problem {
             P2L_M2Pq.erase(P2L_M2Pq.begin() + i);
             --i;
             if (tree[j][nn].P2L[pp].size() != 0) {
+              ++ncompress;
               compress_M2P_P2L(j, pp, nn);
               tree[j][nn].P2L[pp] = Mat();
               tree[j][pp].M2P[nn] = Mat();
@@ -1687,38 +1744,57 @@ struct Problem {
 
   void back_substitution_phase() {  // F:2487-2532
     for (int j = 2; j <= depth; ++j) {
+      if (!(schedule & 1)) {
+        for (int k = nBoxes[j] - 1; k >= 0; --k) back_substitute_box(j, k);
+        continue;
+      }
+      // schedule bit 1: box k reads the particles of its larger-index neighbours
+      // and the multipoles of the others, so wave(k) = 1 + max wave of its
+      // larger-index neighbours orders every read after its write
+      std::vector<int> wave(nBoxes[j], 0);
+      int nw = 0;
       for (int k = nBoxes[j] - 1; k >= 0; --k) {
-        Box& B = tree[j][k];
-        if (B.P2P[k].size() != 0) {
-          ColPivQR qr(B.P2P[k]);
-          Mat rhs1 = B.particle_rhs;
-          for (int n = 0; n < 8; ++n) {
-            int nn = B.neighbors[n];
-            if (nn == -1) continue;
-            if (!tree[j][nn].Eliminated) rhs1 = sub(rhs1, mul(B.P2P[nn], tree[j][nn].particles));
-            else rhs1 = sub(rhs1, mul(B.M2P[nn], tree[j][nn].multipoles));
-          }
-          Mat rhs2 = sub(B.multipoles, mul(B.P2M, qr.solve(rhs1)));
-          Mat Atemp = neg(mul(B.P2M, qr.solve(B.L2P)));
-          if (Atemp.size() != 0) {
-            ColPivQR aq(Atemp);
-            B.locals = aq.solve(rhs2);
-          } else {
-            B.locals = Mat(0, nrhs);
-          }
-          B.particles = qr.solve(sub(rhs1, mul(B.L2P, B.locals)));
-        } else {
-          B.particles = Mat(0, nrhs);
+        for (int n = 0; n < 8; ++n) {
+          int nn = tree[j][k].neighbors[n];
+          if (nn > k) wave[k] = std::max(wave[k], wave[nn] + 1);
         }
-        B.Eliminated = false;
-        if (j != depth) {
-          int o = 0;
-          for (int c = 0; c < 4; ++c) {
-            Box& ch = tree[j + 1][4 * k + c];
-            ch.multipoles = block(B.particles, o, 0, ch.NumMultipoles, nrhs);
-            o += ch.NumMultipoles;
-          }
-        }
+        nw = std::max(nw, wave[k] + 1);
+      }
+      for (int w = 0; w < nw; ++w)
+        for (int k = 0; k < nBoxes[j]; ++k)  // increasing order inside a wave
+          if (wave[k] == w) back_substitute_box(j, k);
+    }
+  }
+  void back_substitute_box(int j, int k) {
+    Box& B = tree[j][k];
+    if (B.P2P[k].size() != 0) {
+      ColPivQR qr(B.P2P[k]);
+      Mat rhs1 = B.particle_rhs;
+      for (int n = 0; n < 8; ++n) {
+        int nn = B.neighbors[n];
+        if (nn == -1) continue;
+        if (!tree[j][nn].Eliminated) rhs1 = sub(rhs1, mul(B.P2P[nn], tree[j][nn].particles));
+        else rhs1 = sub(rhs1, mul(B.M2P[nn], tree[j][nn].multipoles));
+      }
+      Mat rhs2 = sub(B.multipoles, mul(B.P2M, qr.solve(rhs1)));
+      Mat Atemp = neg(mul(B.P2M, qr.solve(B.L2P)));
+      if (Atemp.size() != 0) {
+        ColPivQR aq(Atemp);
+        B.locals = aq.solve(rhs2);
+      } else {
+        B.locals = Mat(0, nrhs);
+      }
+      B.particles = qr.solve(sub(rhs1, mul(B.L2P, B.locals)));
+    } else {
+      B.particles = Mat(0, nrhs);
+    }
+    B.Eliminated = false;
+    if (j != depth) {
+      int o = 0;
+      for (int c = 0; c < 4; ++c) {
+        Box& ch = tree[j + 1][4 * k + c];
+        ch.multipoles = block(B.particles, o, 0, ch.NumMultipoles, nrhs);
+        o += ch.NumMultipoles;
       }
     }
   }
@@ -1775,6 +1851,13 @@ int orc_set_variant(void* h, int full_compress) {
   static_cast<Problem*>(h)->full_compress = full_compress != 0;
   return 0;
 }
+
+int orc_set_schedule(void* h, int flags) {
+  static_cast<Problem*>(h)->schedule = flags;
+  return 0;
+}
+
+long orc_compressions(void* h) { return static_cast<Problem*>(h)->ncompress; }
 
 int orc_grid_points(void* h, double* xy) {
   Problem* P = static_cast<Problem*>(h);

@@ -78,6 +78,13 @@ int orc_set_perturbation(void* h, double rel);
 /* 0: eliminate_phase_efficient (the reference driver's choice, default);
  * 1: eliminate_phase (compress every queued pair after each box). */
 int orc_set_variant(void* h, int full_compress);
+/* Test-only reorderings used by the GPU solver (1: back substitution in waves;
+ * 2: P2P[k][k] factorisation and its right-hand-side / neighbour solves before the
+ * step's recompressions; 4: L2M_f factorisation and its solves before the x-phase
+ * fill-ins).  0 is the reference's order. */
+int orc_set_schedule(void* h, int flags);
+/* recompressions performed by the last solve */
+long orc_compressions(void* h);
 /* dense N x N matrix (column-major complex) implied by the compressed
  * representation before elimination */
 int orc_compressed_dense(const orc_params* p, const double* M, const double* near_tab, double* out);

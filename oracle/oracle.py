@@ -57,6 +57,9 @@ def lib():
         _lib.orc_total_field.argtypes = [v, ctypes.c_int, d, d, d]
         _lib.orc_solve.argtypes = [v, ctypes.c_int, d, d, d]
         _lib.orc_set_variant.argtypes = [v, ctypes.c_int]
+        _lib.orc_set_schedule.argtypes = [v, ctypes.c_int]
+        _lib.orc_compressions.argtypes = [v]
+        _lib.orc_compressions.restype = ctypes.c_long
         _lib.orc_set_perturbation.argtypes = [v, ctypes.c_double]
         _lib.orc_compressed_dense.argtypes = [P(OrcParams), d, d, d]
         _lib.orc_level_ranks.argtypes = [v, ctypes.c_int, i, i]
@@ -130,6 +133,15 @@ class Problem:
 
     def set_variant(self, full_compress):
         lib().orc_set_variant(self.h, 1 if full_compress else 0)
+
+    def set_schedule(self, flags):
+        """Test-only reorderings used by the GPU solver: 1 waves in the back
+        substitution, 2 the P2P[k][k] factorisation before the step's
+        recompressions, 4 the L2M_f factorisation before the x-phase fill-ins."""
+        lib().orc_set_schedule(self.h, int(flags))
+
+    def compressions(self):
+        return int(lib().orc_compressions(self.h))
 
     def set_perturbation(self, rel):
         lib().orc_set_perturbation(self.h, float(rel))

@@ -151,6 +151,26 @@ def test_total_field_satisfies_the_integral_equation(oracle_mod, table_cache, q_
 
 
 @pytest.mark.parametrize("q_kind", ["gauss_aw", "disk"])
+def test_gpu_schedules_change_no_bit(oracle_mod, table_cache, q_kind):
+    """The GPU solver reorders the reference's work: back substitution in waves of
+    non-adjacent boxes; the P2P[k][k] factorisation and its right-hand-side and
+    neighbour solves before the recompressions of step k (second stream); the
+    L2M_f factorisation and its solves before the x-phase fill-ins (second
+    stream).  Restated in the oracle, the reordered schedule gives a bit-identical
+    solution, with recompressions exercised."""
+    p, (M, near, _) = table_cache(depth=4, tol_pow=10, kappa=20.0)
+    p.q_kind = oracle_mod.Q_KINDS[q_kind]
+    xs = []
+    for flags in (0, 1 | 2 | 4):
+        P = oracle_mod.Problem(p, M, near)
+        P.set_schedule(flags)
+        x, _ = P.solve(P.rhs_plane_wave([0.0, 1.1]))
+        assert P.compressions() > 0
+        xs.append(x)
+    assert np.array_equal(xs[0], xs[1])
+
+
+@pytest.mark.parametrize("q_kind", ["gauss_aw", "disk"])
 def test_oracle_elimination_solves_compressed_matrix(oracle_mod, table_cache, q_kind):
     """With every fill-in recompressed (eliminate_phase) the elimination solves the
     compressed matrix to the recompression tolerance; the driver's variant
