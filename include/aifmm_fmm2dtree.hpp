@@ -7,8 +7,12 @@
 #ifndef AIFMM_FMM2DTREE_HPP
 #define AIFMM_FMM2DTREE_HPP
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
+#include <fstream>
+#include <iterator>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -23,6 +27,54 @@ struct pts2D { double x, y; };
 inline void check(aifmm_status s, const aifmm_problem* p) {
   if (s != AIFMM_OK)
     throw std::runtime_error(std::string("aifmm: ") + aifmm_status_string(s) + (p ? std::string(": ") + aifmm_last_error(p) : ""));
+}
+
+// A matrix file of the reference's precomputations/ directory (written with Eigen's
+// operator<<, LS/LS_Assembly.hpp:1166-1184 and :1328-1420), read the way the
+// reference reads it (ReadFromTextFile, :1187-1214): rows = newline count,
+// columns = whitespace-separated tokens / rows, each token a "(re,im)" complex.
+// Returns the entries column-major.
+inline std::vector<dtype> read_eigen_text(const std::string& path, long& rows, long& cols) {
+  std::ifstream in(path);
+  if (!in.good()) throw std::runtime_error("aifmm: cannot open " + path);
+  std::stringstream buf;
+  buf << in.rdbuf();
+  const std::string text = buf.str();
+  rows = (long)std::count(text.begin(), text.end(), '\n');
+  std::istringstream words(text);
+  const long ntok = (long)std::distance(std::istream_iterator<std::string>(words), std::istream_iterator<std::string>());
+  if (rows == 0 || ntok % rows != 0) throw std::runtime_error("aifmm: " + path + " cannot form a matrix");
+  cols = ntok / rows;
+  std::istringstream vals(text);
+  std::vector<dtype> out((size_t)rows * cols);
+  for (long i = 0; i < rows; ++i)
+    for (long j = 0; j < cols; ++j)
+      if (!(vals >> out[(size_t)i + (size_t)j * rows])) throw std::runtime_error("aifmm: bad entry in " + path);
+  return out;
+}
+
+// The leaf-level tables a reference build wrote under root (M_<n>_<depth> and the
+// nine colleagueNeighborInteraction_<depth>_<n> files) in the interleaved layout of
+// aifmm_tables_set: M = 121 x nCheb^2, then nine nCheb^2 x nCheb^2 tables, all
+// column-major.  With them the solver factorises exactly the reference's matrix.
+inline void read_reference_tables(const std::string& root, int nChebNodes, double kappa, int degreeOfBases,
+                                  int depth, std::vector<double>& M, std::vector<double>& near_tables) {
+  const std::string tag = std::to_string(nChebNodes) + "_" + std::to_string(int(kappa)) + "_" +
+                          std::to_string(degreeOfBases);
+  const std::string pre = root + "/precomputations";
+  const long rank = (long)nChebNodes * nChebNodes;
+  long r = 0, c = 0;
+  auto m = read_eigen_text(pre + "/M/M_" + tag + "/M_" + std::to_string(nChebNodes) + "_" + std::to_string(depth), r, c);
+  if (r != 121 || c != rank) throw std::runtime_error("aifmm: M table has the wrong shape");
+  M.assign(reinterpret_cast<const double*>(m.data()), reinterpret_cast<const double*>(m.data()) + 2 * m.size());
+  near_tables.clear();
+  for (int n = 0; n < 9; ++n) {
+    auto t = read_eigen_text(pre + "/Neighbor/Neighbor_" + tag + "/colleagueNeighborInteraction_" +
+                             std::to_string(depth) + "_" + std::to_string(n), r, c);
+    if (r != rank || c != rank) throw std::runtime_error("aifmm: colleague table has the wrong shape");
+    near_tables.insert(near_tables.end(), reinterpret_cast<const double*>(t.data()),
+                       reinterpret_cast<const double*>(t.data()) + 2 * t.size());
+  }
 }
 
 // userkernel (kernel.hpp:90-193).  The reference reads kappa and Qchoice from
@@ -69,6 +121,13 @@ class userkernel {
   }
   std::vector<dtype> getRow(int j, const std::vector<int>& cols) { return getMatrix({j}, cols); }
   std::vector<dtype> getCol(int k, const std::vector<int>& rows) { return getMatrix(rows, {k}); }
+  // readMFromFile + readNeighborInteractions (LS/LS_Assembly.hpp:1216-1228, 1423-1459):
+  // replace the computed tables by the leaf-level files a reference build wrote
+  void readTables(const std::string& root, int nChebNodes, double kappa, int degreeOfBases) {
+    std::vector<double> M, near_tables;
+    read_reference_tables(root, nChebNodes, kappa, degreeOfBases, nLevelsResolve, M, near_tables);
+    check(aifmm_tables_set(p_, M.data(), near_tables.data()), p_);
+  }
   aifmm_problem* handle() { return p_; }
 
  private:

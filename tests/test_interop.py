@@ -53,3 +53,42 @@ def test_rhs_x_files(tmp_path):
     assert os.path.exists(tmp_path / "rhs_x" / "rhs_real_0_10_576.bin")
     assert os.path.exists(tmp_path / "rhs_x" / "rhs_imag_0_10_576.bin")
     assert np.array_equal(interop.read_rhs_x(str(tmp_path), "rhs", 0, 10.0, 576), v)
+
+
+def test_cpp_reader_matches_python_reader(oracle_mod, tmp_path):
+    """include/aifmm_fmm2dtree.hpp reads the reference's table files for C++ users
+    (userkernel::readTables); its values and layout equal the Python reader's."""
+    import shutil
+    import subprocess
+    from aifmm_ls_b200 import interop
+    cxx = shutil.which("g++")
+    if cxx is None:
+        import pytest
+        pytest.skip("no host C++ compiler")
+    p = oracle_mod.params(depth=3, kappa=10.0)
+    M0, N0, _ = oracle_mod.tables(p, round6=False)
+    interop.write_reference_tables(str(tmp_path), p.n_cheb, p.kappa, p.degree, p.depth, M0, N0)
+    src = tmp_path / "read.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include "aifmm_fmm2dtree.hpp"
+int main(int, char** argv) {
+  std::vector<double> M, nt;
+  aifmm::read_reference_tables(argv[1], 6, 10.0, 6, 3, M, nt);
+  FILE* f = std::fopen(argv[2], "wb");
+  std::fwrite(M.data(), sizeof(double), M.size(), f);
+  std::fwrite(nt.data(), sizeof(double), nt.size(), f);
+  std::fclose(f);
+  return 0;
+}
+''')
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = tmp_path / "read"
+    subprocess.check_call([cxx, "-std=c++17", "-O1", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)])
+    out = tmp_path / "tables.bin"
+    subprocess.check_call([str(exe), str(tmp_path), str(out)])
+    raw = np.fromfile(str(out), dtype=np.float64).view(np.complex128)
+    M, N = interop.read_reference_tables(str(tmp_path), p.n_cheb, p.kappa, p.degree, p.depth)
+    r = p.n_cheb ** 2
+    assert np.array_equal(raw[:121 * r], M.ravel(order="F"))
+    assert np.array_equal(raw[121 * r:], np.concatenate([t.ravel(order="F") for t in N]))
