@@ -170,6 +170,28 @@ def test_gpu_schedules_change_no_bit(oracle_mod, table_cache, q_kind):
     assert np.array_equal(xs[0], xs[1])
 
 
+def test_refinement_with_the_compressed_solver_converges(oracle_mod, table_cache):
+    """Iterative refinement against the exact operator, with the solver at a loose
+    recompression tolerance as the inner solve, reaches the exact solution: the
+    plan for the refined factorisation (a loose, fast factor plus residuals of an
+    accurate operator) rests on this contraction."""
+    p, (M, near, _) = table_cache(depth=3, tol_pow=6, kappa=20.0)
+    p.q_kind = oracle_mod.Q_KINDS["gauss_aw"]
+    P = oracle_mod.Problem(p, M, near)
+    A = P.dense()
+    b = P.rhs_plane_wave([0.0])[0]
+    xe = np.linalg.solve(A, b)
+    x = np.zeros_like(b)
+    errs = []
+    for _ in range(5):
+        d, _ = oracle_mod.Problem(p, M, near).solve((b - A @ x)[None, :])
+        x = x + d[0]
+        errs.append(np.linalg.norm(x - xe) / np.linalg.norm(xe))
+    assert errs[0] > 1e-5          # the loose solver alone is far from the solution
+    assert errs[-1] < 1e-10        # five refinement steps reach it
+    assert all(b_ < a for a, b_ in zip(errs, errs[1:]))
+
+
 @pytest.mark.parametrize("q_kind", ["gauss_aw", "disk"])
 def test_oracle_elimination_solves_compressed_matrix(oracle_mod, table_cache, q_kind):
     """With every fill-in recompressed (eliminate_phase) the elimination solves the
