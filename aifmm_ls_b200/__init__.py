@@ -287,10 +287,11 @@ class FMM2DTree:
         return ms
 
     def stats(self):
-        v = np.zeros(13)
-        self._ck(load().aifmm_stats(self.K.h, _dp(v), 13))
+        v = np.zeros(15)
+        self._ck(load().aifmm_stats(self.K.h, _dp(v), 15))
         keys = ["sync_ms", "syncs", "pending_ms", "elim_ms", "back_ms", "compressions", "total_ms", "launches",
-                "asm_lists_ms", "asm_aca_ms", "asm_lu_ms", "asm_blocks_ms", "asm_aca_gpu_ms"]
+                "asm_lists_ms", "asm_aca_ms", "asm_lu_ms", "asm_blocks_ms", "asm_aca_gpu_ms", "pool_bytes",
+                "workspace_bytes"]
         return dict(zip(keys, v.tolist()))
 
     def kernel_profile(self, kind, enable=True):

@@ -12,6 +12,7 @@
 // next: the ACA ranks of a level, the recompression ranks, and the norms that
 // decide which fill-ins are queued for recompression.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cfloat>
 #include <chrono>
@@ -83,7 +84,7 @@ class Pool {
     if (c > (size_t(64) << 20)) {
       void* p = nullptr;
       CK(cudaMalloc(&p, c));
-      big_.push_back(p);
+      big_.push_back({p, c});
       return p;
     }
     if (left_ < c) {
@@ -106,15 +107,20 @@ class Pool {
   }
   void release_all() {
     for (void* p : slabs_) cudaFree(p);
-    for (void* p : big_) cudaFree(p);
+    for (auto& kv : big_) cudaFree(kv.first);
     slabs_.clear(); big_.clear(); free_.clear(); pending_.clear();
     cur_ = nullptr; left_ = 0;
   }
-  size_t reserved() const { return slabs_.size() * (size_t(512) << 20); }
+  size_t reserved() const {
+    size_t b = slabs_.size() * (size_t(512) << 20);
+    for (auto& kv : big_) b += kv.second;
+    return b;
+  }
 
  private:
   static size_t cls(size_t b) { size_t c = 256; while (c < b) c <<= 1; return c; }
-  std::vector<void*> slabs_, big_;
+  std::vector<void*> slabs_;
+  std::vector<std::pair<void*, size_t>> big_;
   std::map<size_t, std::vector<void*>> free_;
   std::vector<std::pair<void*, size_t>> pending_;
   char* cur_ = nullptr;
@@ -138,13 +144,18 @@ class Arena {
   size_t cap_ = 0, off_ = 0;
 };
 
-// Pinned host + device ring for launch descriptors.
+// Pinned host + device ring for launch descriptors.  When the ring wraps, the
+// copies and kernels that read its older slots must have finished: only the
+// handle's own streams use the ring, so those two streams are synchronised
+// (never the whole device).
 class Staging {
  public:
-  void init(size_t bytes) {
+  void init(size_t bytes, cudaStream_t s1, cudaStream_t s2) {
     CK(cudaMallocHost(&h_, bytes));
     CK(cudaMalloc(&d_, bytes));
     cap_ = bytes;
+    s1_ = s1;
+    s2_ = s2;
   }
   ~Staging() {
     if (h_) cudaFreeHost(h_);
@@ -157,7 +168,7 @@ class Staging {
     size_t tot = 0;
     for (auto& p : parts) tot += (p.second + 255) & ~size_t(255);
     if (tot > cap_) throw Fail(AIFMM_ERR_NOMEM, "descriptor batch larger than the staging ring");
-    if (off_ + tot > cap_) { CK(cudaDeviceSynchronize()); off_ = 0; }  // both solver streams
+    if (off_ + tot > cap_) wrap();
     std::vector<const void*> out;
     size_t o = off_;
     for (auto& p : parts) {
@@ -172,16 +183,51 @@ class Staging {
   const void* put_raw(const void* src, size_t bytes, cudaStream_t s) {
     size_t b = (bytes + 255) & ~size_t(255);
     if (b > cap_) throw Fail(AIFMM_ERR_NOMEM, "descriptor batch larger than the staging ring");
-    if (off_ + b > cap_) { CK(cudaDeviceSynchronize()); off_ = 0; }  // both solver streams
+    if (off_ + b > cap_) wrap();
     memcpy(h_ + off_, src, bytes);
     CK(cudaMemcpyAsync(d_ + off_, h_ + off_, bytes, cudaMemcpyHostToDevice, s));
     const void* r = d_ + off_;
     off_ += b;
     return r;
   }
+  void wrap() {
+    if (s1_) CK(cudaStreamSynchronize(s1_));
+    if (s2_) CK(cudaStreamSynchronize(s2_));
+    off_ = 0;
+  }
   char* h_ = nullptr;
   char* d_ = nullptr;
   size_t cap_ = 0, off_ = 0;
+  cudaStream_t s1_ = nullptr, s2_ = nullptr;
+};
+
+// A device buffer that is kept between calls and grows when a larger one is
+// needed (the assembly's per-level ACA workspaces, index lists and LU scratch):
+// after the first assemble of a problem size, no call allocates.  Growing waits
+// for the handle's stream, so that no kernel still reads the old buffer.
+class GrowBuf {
+ public:
+  ~GrowBuf() { if (p_) cudaFree(p_); }
+  void* get(size_t bytes, cudaStream_t s) {
+    bytes = std::max<size_t>(bytes, 256);
+    if (bytes > cap_) {
+      if (p_) {
+        CK(cudaStreamSynchronize(s));
+        CK(cudaFree(p_));
+        p_ = nullptr;
+        cap_ = 0;
+      }
+      const size_t want = std::max(bytes, cap_ + cap_ / 4);
+      CK(cudaMalloc(&p_, want));
+      cap_ = want;
+    }
+    return p_;
+  }
+  size_t capacity() const { return cap_; }
+
+ private:
+  void* p_ = nullptr;
+  size_t cap_ = 0;
 };
 
 struct Blk {
@@ -198,6 +244,7 @@ struct QRF {
   int* info = nullptr;
   double* norms = nullptr;
   bool valid = false;
+  size_t cap[4] = {0, 0, 0, 0};  // bytes of tau, perm, info, norms owned from the pool (0: scratch)
 };
 
 struct Box {
@@ -298,6 +345,7 @@ struct aifmm_problem {
   Pool pool;
   Arena scratch;
   Staging stage;
+  GrowBuf gb_idx, gb_lst, gb_segs, gb_ws, gb_res, gb_lu;
   // timings / counters
   double ms[4] = {0, 0, 0, 0};
   long launches_ = 0, launches_fs = 0, launches_asm = 0;
@@ -337,6 +385,23 @@ struct aifmm_problem {
     b = Blk();
   }
   void assign(Blk& dst, const Blk& src) { drop(dst); dst = src; }
+  // A temporary device buffer from the pool, returned to it when the scope ends
+  // (also when an exception leaves the scope); reuse is ordered by the stream.
+  struct Tmp {
+    aifmm_problem* p; void* ptr; size_t bytes;
+    Tmp(aifmm_problem* p_, size_t b) : p(p_), ptr(p_->pool.alloc(std::max<size_t>(b, 1))), bytes(std::max<size_t>(b, 1)) {}
+    ~Tmp() { p->pool.defer_free(ptr, bytes); }
+    Tmp(const Tmp&) = delete;
+    Tmp& operator=(const Tmp&) = delete;
+    template <class T> T* as() const { return static_cast<T*>(ptr); }
+  };
+  void drop_qrf(QRF& f) {
+    pool.defer_free(f.tau, f.cap[0]);
+    pool.defer_free(f.perm, f.cap[1]);
+    pool.defer_free(f.info, f.cap[2]);
+    pool.defer_free(f.norms, f.cap[3]);
+    f = QRF();
+  }
 
   // ------------------------------------------------------------------ batches
   std::vector<GemmDesc> gd; std::vector<GemmTerm> gt;
@@ -427,10 +492,16 @@ struct aifmm_problem {
     f.qr = A;
     const int n = A.c, s = std::min(A.r, A.c);
     if (persistent) {
-      f.tau = static_cast<double2*>(pool.alloc(sizeof(double2) * std::max(1, s)));
-      f.perm = static_cast<int*>(pool.alloc(sizeof(int) * std::max(1, n)));
-      f.info = static_cast<int*>(pool.alloc(sizeof(int) * 4));
-      f.norms = static_cast<double*>(pool.alloc(sizeof(double) * std::max(1, 2 * n)));
+      drop_qrf(f);
+      f.qr = A;
+      f.cap[0] = sizeof(double2) * std::max(1, s);
+      f.cap[1] = sizeof(int) * std::max(1, n);
+      f.cap[2] = sizeof(int) * 4;
+      f.cap[3] = sizeof(double) * std::max(1, 2 * n);
+      f.tau = static_cast<double2*>(pool.alloc(f.cap[0]));
+      f.perm = static_cast<int*>(pool.alloc(f.cap[1]));
+      f.info = static_cast<int*>(pool.alloc(f.cap[2]));
+      f.norms = static_cast<double*>(pool.alloc(f.cap[3]));
     } else {
       f.tau = static_cast<double2*>(scratch.get(sizeof(double2) * std::max(1, s)));
       f.perm = static_cast<int*>(scratch.get(sizeof(int) * std::max(1, n)));
@@ -635,7 +706,7 @@ struct aifmm_problem {
     N = nleaf * rank;
     nb = d.degree * (d.degree + 1) / 2;
     tol = std::pow(10, -1.0 * d.tol_pow);
-    stage.init(size_t(64) << 20);
+    stage.init(size_t(64) << 20, st, st2);
     scratch.init(size_t(2) << 30);
     CK(cudaMalloc(&d_pts, sizeof(double2) * N));
     CK(cudaMalloc(&d_q, sizeof(double) * N));
@@ -689,27 +760,27 @@ struct aifmm_problem {
     const double* dw = static_cast<const double*>(stage.put_raw(glw, sizeof glw, st));
     const int2* db = stage.put(basis, st);
     const double* dc = stage.put(cheb, st);
-    double2* Cw; double2* Vw; int* status; double* qp;
-    CK(cudaMalloc(&Cw, sizeof(double2) * 121 * nb));
-    CK(cudaMalloc(&Vw, sizeof(double2) * 9 * rank * nb));
-    CK(cudaMalloc(&status, sizeof(int)));
-    CK(cudaMalloc(&qp, sizeof(double) * nb * rank));
-    CK(cudaMemsetAsync(status, 0, sizeof(int), st));
-    KL(aifmm_launch_tables(d.n_cheb, d.degree, d.kappa, r, dx, dw, db, dc, Cw, Vw, status, qp, d_M, d_near, st));
+    Tmp Cw(this, sizeof(double2) * 121 * nb), Vw(this, sizeof(double2) * 9 * rank * nb);
+    Tmp status(this, sizeof(int)), qp(this, sizeof(double) * nb * rank);
+    CK(cudaMemsetAsync(status.ptr, 0, sizeof(int), st));
+    KL(aifmm_launch_tables(d.n_cheb, d.degree, d.kappa, r, dx, dw, db, dc, Cw.as<double2>(), Vw.as<double2>(),
+                           status.as<int>(), qp.as<double>(), d_M, d_near, st));
     int h_status = 0;
-    CK(cudaMemcpyAsync(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&h_status, status.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
     sync();
-    cudaFree(Cw); cudaFree(Vw); cudaFree(status); cudaFree(qp);
     if (h_status) throw Fail(AIFMM_ERR_NUMERIC, "adaptive quadrature exhausted its panel budget");
     if (do_round) {  // the reference's 6-digit text round trip (LS_Assembly.hpp:1178-1228, 1382-1459)
       std::vector<double> M(2 * 121 * rank), Nt(2 * 9 * rank * rank);
-      CK(cudaMemcpy(M.data(), d_M, sizeof(double) * M.size(), cudaMemcpyDeviceToHost));
-      CK(cudaMemcpy(Nt.data(), d_near, sizeof(double) * Nt.size(), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpyAsync(M.data(), d_M, sizeof(double) * M.size(), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(Nt.data(), d_near, sizeof(double) * Nt.size(), cudaMemcpyDeviceToHost, st));
+      sync();
       for (double& v : M) v = round6(v);
       for (double& v : Nt) v = round6(v);
-      CK(cudaMemcpy(d_M, M.data(), sizeof(double) * M.size(), cudaMemcpyHostToDevice));
-      CK(cudaMemcpy(d_near, Nt.data(), sizeof(double) * Nt.size(), cudaMemcpyHostToDevice));
+      CK(cudaMemcpyAsync(d_M, M.data(), sizeof(double) * M.size(), cudaMemcpyHostToDevice, st));
+      CK(cudaMemcpyAsync(d_near, Nt.data(), sizeof(double) * Nt.size(), cudaMemcpyHostToDevice, st));
+      sync();
     }
+    pool.commit_frees();
     tables_ready = true;
     ms[1] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
@@ -717,6 +788,7 @@ struct aifmm_problem {
   // ------------------------------------------------------------------ tree
   void build_tree() {
     auto t0 = std::chrono::steady_clock::now();
+    release_tree();
     T.assign(depth + 1, {});
     nBoxes.assign(depth + 1, 0);
     for (int j = 0; j <= depth; ++j) {
@@ -845,12 +917,9 @@ struct aifmm_problem {
         for (int q = ilb_off[k]; q < ilb_off[k + 1]; ++q) { const int b = ilb[q]; in.n2 += lout_len(b); seg(lout_off[b], lout_len(b)); }
       }
       if (cur_i > INT_MAX || (long)lst.size() > INT_MAX) throw Fail(AIFMM_ERR_NOMEM, "ACA index lists too long");
-      int* d_idx = nullptr;
-      int* d_lst = nullptr;
-      int4* d_segs = nullptr;
-      CK(cudaMalloc(&d_idx, sizeof(int) * std::max<long>(1, cur_i)));
-      CK(cudaMalloc(&d_lst, sizeof(int) * std::max<size_t>(1, lst.size())));
-      CK(cudaMalloc(&d_segs, sizeof(int4) * std::max<size_t>(1, segs.size())));
+      int* d_idx = static_cast<int*>(gb_idx.get(sizeof(int) * std::max<long>(1, cur_i), st));
+      int* d_lst = static_cast<int*>(gb_lst.get(sizeof(int) * std::max<size_t>(1, lst.size()), st));
+      int4* d_segs = static_cast<int4*>(gb_segs.get(sizeof(int4) * std::max<size_t>(1, segs.size()), st));
       if (!lst.empty()) CK(cudaMemcpyAsync(d_lst, lst.data(), sizeof(int) * lst.size(), cudaMemcpyHostToDevice, st));
       if (!segs.empty()) {
         CK(cudaMemcpyAsync(d_segs, segs.data(), sizeof(int4) * segs.size(), cudaMemcpyHostToDevice, st));
@@ -868,10 +937,9 @@ struct aifmm_problem {
         ro[t] = nres;
         nres += 2 * (size_t)rmax;
       }
-      char* d_ws = nullptr;
-      int* d_res = nullptr;  // [2 per job: rank, branch] then the bases
-      CK(cudaMalloc(&d_ws, std::max<size_t>(ws, 256)));
-      CK(cudaMalloc(&d_res, sizeof(int) * (2 * (size_t)2 * nbx + nres + 1)));
+      char* d_ws = static_cast<char*>(gb_ws.get(ws, st));
+      // [2 per job: rank, branch] then the bases
+      int* d_res = static_cast<int*>(gb_res.get(sizeof(int) * (2 * (size_t)2 * nbx + nres + 1), st));
       int* d_bases = d_res + 2 * 2 * nbx;
       std::vector<AcaJob> jobs(2 * nbx);
       for (int t = 0; t < 2 * nbx; ++t) {
@@ -924,11 +992,6 @@ struct aifmm_problem {
         CK(cudaEventElapsedTime(&ms_, ea, eb));
         st_asm_aca_gpu_ms += ms_;
       }
-      cudaFree(d_res);
-      cudaFree(d_ws);
-      cudaFree(d_idx);
-      cudaFree(d_lst);
-      cudaFree(d_segs);
       st_asm_aca_ms += since(ta);
       ta = clk::now();
       // ---- skeletons, rank equalisation (F:1105-1113) and L2P / P2M jobs
@@ -993,9 +1056,8 @@ struct aifmm_problem {
         lws += (sizeof(double2) * ((size_t)r * r + (size_t)r * m_out) + sizeof(int) * r + 511) & ~size_t(255);
         lj.push_back(b);
       }
-      char* d_lw = nullptr;
       if (!lj.empty()) {
-        CK(cudaMalloc(&d_lw, lws));
+        char* d_lw = static_cast<char*>(gb_lu.get(lws, st));
         for (size_t t = 0; t < lj.size(); ++t) {
           char* base = d_lw + lwo[t];
           const int r = lj[t].r, m = lj[t].m;
@@ -1005,7 +1067,6 @@ struct aifmm_problem {
         const SkelLUJob* dl = stage.put(lj, st);
         KL(aifmm_launch_skel_lu(dl, (int)lj.size(), cx, st));
         sync();
-        cudaFree(d_lw);
       }
       for (int k = 0; k < nbx; ++k) { Box& B = T[j][k]; drop(B.Ac); drop(B.Ar); }
       pool.commit_frees();
@@ -1996,9 +2057,24 @@ struct aifmm_problem {
         drop(B.L2P_f); drop(B.L2M_f); drop(B.prhs); drop(B.mrhs); drop(B.lrhs); drop(B.locals);
         drop(B.particles);
         drop(B.multipoles);
-        B.qx = QRF(); B.qz = QRF();
+        drop_qrf(B.qx); drop_qrf(B.qz);
         B.elim = false;
       }
+  }
+  // Everything a tree holds, before the tree is rebuilt: the elimination's blocks
+  // and factorisations, the bases, the ACA factors and the kept copy of the
+  // assembly.
+  void release_tree() {
+    CK(cudaStreamSynchronize(st));
+    CK(cudaStreamSynchronize(st2));
+    if (have_saved) release_saved();
+    have_saved = false;
+    consumed = false;
+    assembled = false;
+    release_level_data();
+    for (auto& lv : T)
+      for (auto& B : lv) { drop(B.L2P); drop(B.P2M); drop(B.Ac); drop(B.Ar); }
+    pool.commit_frees();
   }
 
   bool consumed = false;  // the elimination consumed the assembled blocks
@@ -2135,18 +2211,20 @@ namespace {
 constexpr size_t kTablesScratchBytes = size_t(1) << 20;  // 1 MiB
 __device__ __align__(256) unsigned char g_tables_scratch[kTablesScratchBytes];
 constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {nullptr};
+std::atomic<void*> g_scratch_addr[kMaxDevices];
 }  // namespace
 
 extern "C" aifmm_status aifmm_tables_compute_noalloc(aifmm_problem* p, double* M_dev, double* near_dev) {
   if (!p || !M_dev || !near_dev) return AIFMM_ERR_ARG;
-  if (cudaSetDevice(p->device) != cudaSuccess) return AIFMM_ERR_CUDA;
   if (p->device < 0 || p->device >= kMaxDevices) return AIFMM_ERR_ARG;
-  // the symbol's device address, looked up once per device with that device current
-  void*& base = g_scratch_addr[p->device];
+  if (cudaSetDevice(p->device) != cudaSuccess) return AIFMM_ERR_CUDA;
+  // the symbol's device address, looked up once per device with that device
+  // current (threads that race here all store the same address)
+  void* base = g_scratch_addr[p->device].load(std::memory_order_acquire);
   if (!base) {
     void* ptr = nullptr;
     if (cudaGetSymbolAddress(&ptr, g_tables_scratch) != cudaSuccess || !ptr) return AIFMM_ERR_CUDA;
+    g_scratch_addr[p->device].store(ptr, std::memory_order_release);
     base = ptr;
   }
   const int rank = p->rank, nb = p->nb;
@@ -2301,15 +2379,13 @@ aifmm_status aifmm_rhs_plane_wave(aifmm_problem* p, int nrhs, const double* thet
   return guard(p, [&] {
     const double* dth = static_cast<const double*>(p->stage.put_raw(theta, sizeof(double) * nrhs, p->st));
     const size_t bytes = sizeof(double2) * (size_t)p->N * nrhs;
-    double2* db = (flags & AIFMM_PTR_DEVICE) ? reinterpret_cast<double2*>(b) : nullptr;
-    if (!db) CK(cudaMalloc(&db, bytes));
+    const bool dev = flags & AIFMM_PTR_DEVICE;
+    aifmm_problem::Tmp tb(p, dev ? 1 : bytes);
+    double2* db = dev ? reinterpret_cast<double2*>(b) : tb.as<double2>();
     int e = aifmm_launch_rhs_plane_wave(p->d_pts, p->d_q, p->d.kappa, p->N, nrhs, dth, db, p->st);
     if (e) throw Fail(AIFMM_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
-    if (!(flags & AIFMM_PTR_DEVICE)) {
-      CK(cudaMemcpyAsync(b, db, bytes, cudaMemcpyDeviceToHost, p->st));
-      p->sync();
-      cudaFree(db);
-    }
+    if (!dev) CK(cudaMemcpyAsync(b, db, bytes, cudaMemcpyDeviceToHost, p->st));
+    p->sync();
   });
 }
 
@@ -2321,23 +2397,20 @@ aifmm_status aifmm_entries(aifmm_problem* p, long n, const int* I, const int* J,
     const bool dev = flags & AIFMM_PTR_DEVICE;
     const int *dI = I, *dJ = J;
     double2* dO = reinterpret_cast<double2*>(out);
-    int *tI = nullptr, *tJ = nullptr;
-    double2* tO = nullptr;
-    if (!dev) {
+    if (!dev)
       for (long t = 0; t < n; ++t)
         if (I[t] < 0 || I[t] >= p->N || J[t] < 0 || J[t] >= p->N) throw Fail(AIFMM_ERR_ARG, "point index out of range");
-      CK(cudaMalloc(&tI, sizeof(int) * n)); CK(cudaMalloc(&tJ, sizeof(int) * n)); CK(cudaMalloc(&tO, sizeof(double2) * n));
-      CK(cudaMemcpyAsync(tI, I, sizeof(int) * n, cudaMemcpyHostToDevice, p->st));
-      CK(cudaMemcpyAsync(tJ, J, sizeof(int) * n, cudaMemcpyHostToDevice, p->st));
-      dI = tI; dJ = tJ; dO = tO;
+    aifmm_problem::Tmp tI(p, dev ? 1 : sizeof(int) * n), tJ(p, dev ? 1 : sizeof(int) * n);
+    aifmm_problem::Tmp tO(p, dev ? 1 : sizeof(double2) * n);
+    if (!dev) {
+      CK(cudaMemcpyAsync(tI.ptr, I, sizeof(int) * n, cudaMemcpyHostToDevice, p->st));
+      CK(cudaMemcpyAsync(tJ.ptr, J, sizeof(int) * n, cudaMemcpyHostToDevice, p->st));
+      dI = tI.as<int>(); dJ = tJ.as<int>(); dO = tO.as<double2>();
     }
     int e = aifmm_launch_list_entries(dI, dJ, n, dO, p->ctx(), p->st);
     if (e) throw Fail(AIFMM_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
-    if (!dev) {
-      CK(cudaMemcpyAsync(out, tO, sizeof(double2) * n, cudaMemcpyDeviceToHost, p->st));
-      p->sync();
-      cudaFree(tI); cudaFree(tJ); cudaFree(tO);
-    }
+    if (!dev) CK(cudaMemcpyAsync(out, dO, sizeof(double2) * n, cudaMemcpyDeviceToHost, p->st));
+    p->sync();
   });
 }
 
@@ -2388,21 +2461,15 @@ aifmm_status aifmm_dense_matvec(aifmm_problem* p, int nrhs, const double* x, dou
     const bool dev = flags & AIFMM_PTR_DEVICE;
     const double2* dx = reinterpret_cast<const double2*>(x);
     double2* dy = reinterpret_cast<double2*>(y);
-    double2 *tx = nullptr, *ty = nullptr;
+    aifmm_problem::Tmp tx(p, dev ? 1 : bytes), ty(p, dev ? 1 : bytes);
     if (!dev) {
-      CK(cudaMalloc(&tx, bytes)); CK(cudaMalloc(&ty, bytes));
-      CK(cudaMemcpyAsync(tx, x, bytes, cudaMemcpyHostToDevice, p->st));
-      dx = tx; dy = ty;
+      CK(cudaMemcpyAsync(tx.ptr, x, bytes, cudaMemcpyHostToDevice, p->st));
+      dx = tx.as<double2>(); dy = ty.as<double2>();
     }
     int e = aifmm_launch_dense_matvec(dx, dy, p->N, nrhs, p->ctx(), p->st);
     if (e) throw Fail(AIFMM_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
-    if (!dev) {
-      CK(cudaMemcpyAsync(y, ty, bytes, cudaMemcpyDeviceToHost, p->st));
-      p->sync();
-      cudaFree(tx); cudaFree(ty);
-    } else {
-      p->sync();
-    }
+    if (!dev) CK(cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, p->st));
+    p->sync();
   });
 }
 
@@ -2415,23 +2482,17 @@ aifmm_status aifmm_total_field(aifmm_problem* p, int nrhs, const double* theta, 
     const bool dev = flags & AIFMM_PTR_DEVICE;
     const double2* dphi = reinterpret_cast<const double2*>(phi);
     double2* du = reinterpret_cast<double2*>(u);
-    double2 *tphi = nullptr, *tu = nullptr;
+    aifmm_problem::Tmp tphi(p, dev ? 1 : bytes), tu(p, dev ? 1 : bytes);
     if (!dev) {
-      CK(cudaMalloc(&tphi, bytes)); CK(cudaMalloc(&tu, bytes));
-      CK(cudaMemcpyAsync(tphi, phi, bytes, cudaMemcpyHostToDevice, p->st));
-      dphi = tphi; du = tu;
+      CK(cudaMemcpyAsync(tphi.ptr, phi, bytes, cudaMemcpyHostToDevice, p->st));
+      dphi = tphi.as<double2>(); du = tu.as<double2>();
     }
     const double* dth = static_cast<const double*>(p->stage.put_raw(theta, sizeof(double) * nrhs, p->st));
     int e = aifmm_launch_incident_field(p->d_pts, p->d.kappa, p->N, nrhs, dth, du, p->st);
     if (!e) e = aifmm_launch_green_matvec_add(dphi, du, p->N, nrhs, p->ctx(), p->st);
     if (e) throw Fail(AIFMM_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
-    if (!dev) {
-      CK(cudaMemcpyAsync(u, tu, bytes, cudaMemcpyDeviceToHost, p->st));
-      p->sync();
-      cudaFree(tphi); cudaFree(tu);
-    } else {
-      p->sync();
-    }
+    if (!dev) CK(cudaMemcpyAsync(u, du, bytes, cudaMemcpyDeviceToHost, p->st));
+    p->sync();
   });
 }
 
@@ -2486,11 +2547,13 @@ aifmm_status aifmm_kernel_profile_read(aifmm_problem* p, int kind, long* launche
 
 aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n) {
   if (!p || !out) return AIFMM_ERR_ARG;
-  const double v[13] = {p->st_sync_ms, (double)p->st_syncs, p->st_pending_ms, p->st_elim_ms, p->st_back_ms,
+  const double grow = (double)(p->gb_idx.capacity() + p->gb_lst.capacity() + p->gb_segs.capacity() +
+                               p->gb_ws.capacity() + p->gb_res.capacity() + p->gb_lu.capacity());
+  const double v[15] = {p->st_sync_ms, (double)p->st_syncs, p->st_pending_ms, p->st_elim_ms, p->st_back_ms,
                         (double)p->st_compress, p->ms[3], (double)p->launches_fs,
                         p->st_asm_lists_ms, p->st_asm_aca_ms, p->st_asm_lu_ms, p->st_asm_blocks_ms,
-                        p->st_asm_aca_gpu_ms};
-  for (int i = 0; i < n && i < 13; ++i) out[i] = v[i];
+                        p->st_asm_aca_gpu_ms, (double)p->pool.reserved(), grow};
+  for (int i = 0; i < n && i < 15; ++i) out[i] = v[i];
   return AIFMM_OK;
 }
 

@@ -155,7 +155,8 @@ aifmm_status aifmm_kernel_profile_read(aifmm_problem* p, int kind, long* launche
  * [7] kernel launches; of the last assemble: [8] ms building index lists on the host,
  * [9] ms in the ACA (launch to ranks on the host), [10] ms for the interpolative
  * operators, [11] ms for the M2L and P2P block entries, [12] ms of ACA kernel time
- * (CUDA events).  n <= 13 values are written. */
+ * (CUDA events); device memory held by the handle: [13] bytes of the block pool, [14] bytes
+ * of the assembly's reusable workspaces.  n <= 15 values are written. */
 aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n);
 /* The CUDA stream the handle works on (cudaStream_t). */
 aifmm_status aifmm_get_stream(const aifmm_problem* p, void** stream);

@@ -198,3 +198,62 @@ def test_total_field_matches_oracle(oracle_mod, table_cache):
     # this compression tolerance (the oracle's own solution gives the same)
     q = P.contrast()
     assert np.linalg.norm(p.kappa ** 2 * q * u + phi) / np.linalg.norm(phi) <= 1e-3
+
+
+def test_reference_default_run_depth5(oracle_mod, table_cache):
+    """The reference's default run `testFMM2D_find_error 6 10 6 1 0 8 5`
+    (testFMM2D_find_error.cpp:44-52, Readme.md:17-21): 6x6 nodes, kappa 10,
+    degree 6, Qchoice 0, TOL 1e-8, depth 5 (36,864 unknowns), one plane wave at
+    theta = 0.  The GPU solution matches the oracle's to the flat 1e-8."""
+    import aifmm_ls_b200 as A
+    p, tabs = table_cache(depth=5, q_kind="gaussian160", kappa=10.0, tol_pow=8)
+    M, near = tabs[:2]
+    K = _kernel(p, tabs)
+    T = A.FMM2DTree(K)
+    T.createTree()
+    T.assemble()
+    P = oracle_mod.Problem(p, M, near)
+    b = P.rhs_plane_wave([0.0])
+    xo, _ = P.solve(b)
+    x = T.solve(b)
+    rel = np.linalg.norm(x - xo) / np.linalg.norm(xo)
+    print("depth 5 reference run: |x_gpu - x_oracle| / |x_oracle| = %.2e" % rel)
+    assert rel <= SOLVE_TOL
+
+
+def test_bench_path_with_gpu_tables(oracle_mod):
+    """The benchmark's own path: tables computed on the GPU with the 6-digit round
+    trip, against the oracle with the tables it computes itself (benchmark
+    physics at depth 4: Gaussian 1.5 exp(-32|x|^2), kappa 40, TOL 1e-10)."""
+    import aifmm_ls_b200 as A
+    kw = dict(n_cheb=6, kappa=40.0, degree=6, depth=4, tol_pow=10, q_kind="gauss_aw", q_amp=1.5, q_width=32.0)
+    p = oracle_mod.params(**kw)
+    M0, N0, _ = oracle_mod.tables(p, round6=False)
+    M0r, N0r, _ = oracle_mod.tables(p, round6=True)
+    K = A.LSKernel(**kw)
+    K.tables_compute(round6=False)
+    M1, N1 = K.tables_get()
+    K.tables_compute(round6=True)
+    M1r, N1r = K.tables_get()
+    v0 = np.concatenate([M0.ravel(), N0.ravel()])
+    v1 = np.concatenate([M1.ravel(), N1.ravel()])
+    w0 = np.concatenate([M0r.ravel(), N0r.ravel()])
+    w1 = np.concatenate([M1r.ravel(), N1r.ravel()])
+    ok = np.abs(v0) > 0
+    rel_unrounded = np.max(np.abs(v1 - v0)[ok] / np.abs(v0)[ok])
+    flips = int(np.count_nonzero(w0 != w1))
+    print("tables before rounding: max relative difference %.2e; 6-digit values differing: %d of %d"
+          % (rel_unrounded, flips, w0.size))
+    T = A.FMM2DTree(K)
+    T.createTree()
+    T.assemble()
+    th = [0.0, 2.1]
+    b = K.rhs_plane_wave(th)
+    x = T.solve(b)
+    P = oracle_mod.Problem(p, M0r, N0r)
+    xo, _ = P.solve(b)
+    rel = np.linalg.norm(x - xo) / np.linalg.norm(xo)
+    spread = _oracle_spread(oracle_mod, p, M0r, N0r, b, xo)
+    print("bench path: |x_gpu(gpu tables) - x_oracle(oracle tables)| = %.2e, oracle spread %.2e" % (rel, spread))
+    assert rel_unrounded <= 1e-9
+    assert rel <= max(SOLVE_TOL, 5.0 * spread, 1e-6), (rel, spread)
