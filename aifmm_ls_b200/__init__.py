@@ -17,13 +17,14 @@ import os
 
 import numpy as np
 
-__all__ = ["AifmmError", "LSKernel", "FMM2DTree", "Desc", "load", "lib_path", "Q_KINDS"]
+__all__ = ["AifmmError", "LSKernel", "FMM2DTree", "Server", "Desc", "load", "lib_path", "Q_KINDS"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "lib", "libaifmm_b200.so")
 _lib = None
 
 PTR_HOST, PTR_DEVICE, KEEP_ASSEMBLY = 0, 1, 2
+PRECISION_FP64 = 0
 Q_KINDS = {"gaussian160": 0, "multi_gauss": 1, "plasma": 2, "flatbump": 3, "cavity": 4, "lens": 5,
            "gauss_aw": 10, "disk": 11}
 
@@ -64,6 +65,23 @@ SIGNATURES = {
     "aifmm_build_tree": ([_v], ctypes.c_int),
     "aifmm_assemble": ([_v], ctypes.c_int),
     "aifmm_factorize_solve": ([_v, ctypes.c_int, _d, _d, ctypes.c_int], ctypes.c_int),
+    "aifmm_factorize": ([_v, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "aifmm_solve": ([_v, ctypes.c_int, _d, ctypes.c_long, _d, ctypes.c_long, _v, ctypes.c_int], ctypes.c_int),
+    "aifmm_find_error": ([_v, ctypes.c_int, _d, ctypes.c_long, _d, ctypes.c_long, _d, ctypes.c_int], ctypes.c_int),
+    "aifmm_zgemm": ([_v, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, _d, ctypes.c_int,
+                     _d, ctypes.c_int, _d, _d, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+    "aifmm_trim": ([_v], ctypes.c_int),
+    "aifmm_set_factor_tolerance": ([_v, ctypes.c_int], ctypes.c_int),
+    "aifmm_compressed_matvec": ([_v, ctypes.c_int, _d, ctypes.c_long, _d, ctypes.c_long, ctypes.c_int], ctypes.c_int),
+    "aifmm_solve_refined": ([_v, ctypes.c_int, _d, ctypes.c_long, _d, ctypes.c_long, ctypes.c_double, ctypes.c_int,
+                             _i, _d, ctypes.c_int], ctypes.c_int),
+    "aifmm_server_create": ([ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _P(_v)], ctypes.c_int),
+    "aifmm_server_destroy": ([_v], ctypes.c_int),
+    "aifmm_server_factorize": ([_v, ctypes.c_longlong, _P(Desc), _P(ctypes.c_long)], ctypes.c_int),
+    "aifmm_server_solve": ([_v, ctypes.c_longlong, ctypes.c_int, _d, _d, _P(ctypes.c_long)], ctypes.c_int),
+    "aifmm_server_wait": ([_v, ctypes.c_long, ctypes.c_double, _i, _d, _i], ctypes.c_int),
+    "aifmm_server_stats": ([_v, _d, ctypes.c_int], ctypes.c_int),
+    "aifmm_launch_counts_split": ([_v, _P(ctypes.c_long), _P(ctypes.c_long)], ctypes.c_int),
     "aifmm_dense_matvec": ([_v, ctypes.c_int, _d, _d, ctypes.c_int], ctypes.c_int),
     "aifmm_total_field": ([_v, ctypes.c_int, _d, _d, _d, ctypes.c_int], ctypes.c_int),
     "aifmm_level_ranks": ([_v, ctypes.c_int, _i, _i], ctypes.c_int),
@@ -201,6 +219,21 @@ class LSKernel:
     def getCol(self, k, rows):
         return self.getMatrix(rows, [k])[:, 0]
 
+    def zgemm(self, A, B, C=None, alpha=1.0, beta=0.0, opA=0, opB=0):
+        """C = alpha op(A) op(B) + beta C with the solver's batched GEMM kernel (op 1 = conjugate transpose)."""
+        A = np.asfortranarray(A, dtype=np.complex128)
+        B = np.asfortranarray(B, dtype=np.complex128)
+        m = A.shape[1] if opA else A.shape[0]
+        k = A.shape[0] if opA else A.shape[1]
+        n = B.shape[0] if opB else B.shape[1]
+        C = np.zeros((m, n), np.complex128, order="F") if C is None else np.asfortranarray(C, dtype=np.complex128).copy(order="F")
+        al = np.array([complex(alpha)], np.complex128).view(np.float64)
+        be = np.array([complex(beta)], np.complex128).view(np.float64)
+        self._ck(load().aifmm_zgemm(self.h, opA, opB, m, n, k, _dp(al), _dp(A.ravel(order="F").view(np.float64)),
+                                    max(1, A.shape[0]), _dp(B.ravel(order="F").view(np.float64)), max(1, B.shape[0]),
+                                    _dp(be), _dp(C.ravel(order="K").view(np.float64)), max(1, m), PTR_HOST))
+        return C
+
     def dense_matvec(self, x):
         """y = A x with exact entries (the find_error fixture product); x: (nrhs, N)."""
         x = np.atleast_2d(np.asarray(x, dtype=np.complex128))
@@ -262,10 +295,56 @@ class FMM2DTree:
         self.x = x
         return x
 
+    # eliminate_phase_efficient + the base-level factorisation, right-hand side not carried (F:2407-2485)
+    def factorize(self, keep_assembly=False):
+        self._ck(load().aifmm_factorize(self.K.h, PRECISION_FP64, KEEP_ASSEMBLY if keep_assembly else 0))
+
+    def set_factor_tolerance(self, tol_pow):
+        """recompression tolerance 10^-tol_pow of the next factorisations (0: the problem's)"""
+        self._ck(load().aifmm_set_factor_tolerance(self.K.h, tol_pow))
+
+    def compressed_matvec(self, x):
+        """y = A_c x with the kept pre-elimination assembly (factorize(keep_assembly=True) first)"""
+        x = np.ascontiguousarray(np.atleast_2d(np.asarray(x, np.complex128)))
+        y = np.zeros_like(x)
+        N = self.K.N
+        self._ck(load().aifmm_compressed_matvec(self.K.h, x.shape[0], _dp(x.view(np.float64)), N,
+                                                _dp(y.view(np.float64)), N, PTR_HOST))
+        return y
+
+    def solve_refined(self, b, rtol=1e-10, maxit=60):
+        """GMRES on A_c x = b preconditioned by the kept factors; returns (x, iterations, relres)"""
+        b = np.ascontiguousarray(np.atleast_2d(np.asarray(b, np.complex128)))
+        x = np.zeros_like(b)
+        N = self.K.N
+        it = ctypes.c_int()
+        rr = ctypes.c_double()
+        self._ck(load().aifmm_solve_refined(self.K.h, b.shape[0], _dp(b.view(np.float64)), N, _dp(x.view(np.float64)),
+                                            N, float(rtol), int(maxit), ctypes.byref(it), ctypes.byref(rr), PTR_HOST))
+        self.x = x
+        return x, it.value, rr.value
+
+    # the right-hand-side half with kept factors (F:1968-2001, 2252-2293, 2453-2532)
+    def solve_factored(self, b):
+        b = np.ascontiguousarray(np.atleast_2d(np.asarray(b, np.complex128)))
+        x = np.zeros_like(b)
+        N = self.K.N
+        self._ck(load().aifmm_solve(self.K.h, b.shape[0], _dp(b.view(np.float64)), N, _dp(x.view(np.float64)), N,
+                                    None, PTR_HOST))
+        self.x = x
+        return x
+
     def error_check(self, x_true):
-        """relative forward error ||x - x_true|| / ||x_true|| (F:2534-2581)"""
-        x_true = np.atleast_2d(x_true)
-        return float(np.linalg.norm(self.x - x_true) / np.linalg.norm(x_true))
+        """relative forward error ||x - x_true|| / ||x_true|| (F:2534-2581), through the C ABI"""
+        x_true = np.ascontiguousarray(np.atleast_2d(np.asarray(x_true, np.complex128)))
+        x = np.ascontiguousarray(self.x)
+        if x.shape != x_true.shape:
+            raise ValueError("solution and reference have different shapes")
+        rel = ctypes.c_double()
+        N = self.K.N
+        self._ck(load().aifmm_find_error(self.K.h, x.shape[0], _dp(x.view(np.float64)), N,
+                                         _dp(x_true.view(np.float64)), N, ctypes.byref(rel), PTR_HOST))
+        return rel.value
 
     def level_ranks(self, level):
         n = 4 ** level
@@ -282,7 +361,7 @@ class FMM2DTree:
         return out[:cnt.value].copy()
 
     def phase_times(self):
-        ms = np.zeros(4)
+        ms = np.zeros(6)
         self._ck(load().aifmm_phase_times(self.K.h, _dp(ms)))
         return ms
 
@@ -304,8 +383,82 @@ class FMM2DTree:
         self._ck(load().aifmm_kernel_profile_read(self.K.h, kind, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(fl)))
         return n.value, ms.value, fl.value
 
+    def launch_counts_split(self):
+        a = ctypes.c_long()
+        b = ctypes.c_long()
+        self._ck(load().aifmm_launch_counts_split(self.K.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def launch_counts(self):
         a = ctypes.c_long()
         b = ctypes.c_long()
         self._ck(load().aifmm_launch_counts(self.K.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+
+class Server:
+    """The serving loop of the C ABI (aifmm_server_*): factorisations kept on the
+    device under keys, continuous batching of solve requests, admission by device
+    memory with LRU eviction.  Requests return ids; ``wait`` returns the result."""
+
+    STAT_KEYS = ["solve_p50_ms", "solve_p99_ms", "factorize_p50_ms", "factorize_p99_ms", "solves", "factorizations",
+                 "evictions", "batches", "mean_batch_rhs", "bytes_in_use", "resident", "failed"]
+
+    def __init__(self, device=0, hbm_budget_bytes=0.0, workers=2, max_batch_rhs=64):
+        h = _v()
+        st = load().aifmm_server_create(device, float(hbm_budget_bytes), workers, max_batch_rhs, ctypes.byref(h))
+        if st != 0:
+            raise AifmmError(st, load().aifmm_status_string(st).decode())
+        self.h = h
+        self._bufs = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().aifmm_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def factorize(self, key, n_cheb=6, kappa=10.0, degree=6, L=1.0, depth=5, tol_pow=8, q_kind="gaussian160",
+                  q_amp=1.5, q_width=32.0, q_radius=0.5):
+        k = Q_KINDS[q_kind] if isinstance(q_kind, str) else int(q_kind)
+        d = Desc(n_cheb, float(kappa), degree, float(L), depth, tol_pow, k, float(q_amp), float(q_width),
+                 float(q_radius))
+        rid = ctypes.c_long()
+        st = load().aifmm_server_factorize(self.h, key, ctypes.byref(d), ctypes.byref(rid))
+        if st != 0:
+            raise AifmmError(st, "factorize request refused")
+        return rid.value
+
+    def solve(self, key, b):
+        """b: (nrhs, N) complex; returns the request id (the solution comes from wait)."""
+        b = np.ascontiguousarray(np.atleast_2d(np.asarray(b, np.complex128)))
+        x = np.zeros_like(b)
+        rid = ctypes.c_long()
+        st = load().aifmm_server_solve(self.h, key, b.shape[0], _dp(b.view(np.float64)), _dp(x.view(np.float64)),
+                                       ctypes.byref(rid))
+        if st != 0:
+            raise AifmmError(st, "solve request refused")
+        self._bufs[rid.value] = (b, x)  # kept alive until wait()
+        return rid.value
+
+    def wait(self, rid, timeout=600.0):
+        """Returns (status, latency_ms, batch_rhs, x or None)."""
+        res = ctypes.c_int()
+        lat = ctypes.c_double()
+        br = ctypes.c_int()
+        st = load().aifmm_server_wait(self.h, rid, float(timeout), ctypes.byref(res), ctypes.byref(lat),
+                                      ctypes.byref(br))
+        if st != 0:
+            raise AifmmError(st, "request %d not finished or unknown" % rid)
+        bufs = self._bufs.pop(rid, None)
+        return res.value, lat.value, br.value, (bufs[1] if bufs is not None else None)
+
+    def stats(self):
+        v = np.zeros(12)
+        load().aifmm_server_stats(self.h, _dp(v), 12)
+        return dict(zip(self.STAT_KEYS, v.tolist()))

@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libaifmm_b200.so")
-SOURCES = ["k_geom.cu", "k_tables.cu", "k_entries.cu", "k_aca.cu", "k_dense.cu", "solver.cu"]
+SOURCES = ["k_geom.cu", "k_tables.cu", "k_entries.cu", "k_aca.cu", "k_dense.cu", "solver.cu", "server.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -48,7 +48,7 @@ def build(verbose=False, jobs=None):
     procs = []
     objs = []
     for s in srcs:
-        o = os.path.join(objdir, os.path.basename(s).replace(".cu", ".o"))
+        o = os.path.join(objdir, os.path.splitext(os.path.basename(s))[0] + ".o")
         objs.append(o)
         cmd = [nvcc()] + flags + ["-c", s, "-o", o]
         if verbose:
@@ -61,7 +61,7 @@ def build(verbose=False, jobs=None):
         if verbose and out:
             print(out.decode(errors="replace"))
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + ARCH + ["-shared", "-ccbin", _host_cxx(), "-o", tmp] + objs + ["-lcudart"]
+    cmd = [nvcc()] + ARCH + ["-shared", "-ccbin", _host_cxx(), "-o", tmp] + objs + ["-lcudart", "-lpthread"]
     subprocess.check_call(cmd)
     os.replace(tmp, LIB)
     # the reference driver's command line, on the C++ surface of include/aifmm_fmm2dtree.hpp

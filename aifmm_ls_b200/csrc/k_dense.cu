@@ -699,6 +699,13 @@ __device__ __forceinline__ void gemm_fetch(const GemmTerm& T, int k0, int row0, 
     if (gj < n && gkb < T.k) rb[u] = T.opB ? cconj(T.B[gj + (size_t)gkb * T.ldb]) : T.B[gkb + (size_t)gj * T.ldb];
   }
 }
+// d += a b for one m8n8k4 FP64 tensor-core product (each lane: one A element,
+// one B element, two accumulators)
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
 __global__ void __launch_bounds__(256) gemm_kernel(const GemmDesc* __restrict__ ds, const GemmTerm* __restrict__ terms,
                                                    const int* __restrict__ tile_off, int nd) {
   const int bid = blockIdx.x;
@@ -710,9 +717,9 @@ __global__ void __launch_bounds__(256) gemm_kernel(const GemmDesc* __restrict__ 
   const int tm = t % tiles_m, tn = t / tiles_m;
   __shared__ double2 As[TK][TM + 1];
   __shared__ double2 Bs[TK][TN + 1];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double2 acc[2][2];
-  for (int a = 0; a < 2; ++a) for (int b = 0; b < 2; ++b) acc[a][b] = make_double2(0.0, 0.0);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int si = warp & 3, sj0 = 2 * (warp >> 2);
+  double cr[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, ci[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
   const int row0 = tm * TM, col0 = tn * TN;
   int tt = 0, k0 = 0;
   GemmTerm T{};
@@ -737,25 +744,36 @@ __global__ void __launch_bounds__(256) gemm_kernel(const GemmDesc* __restrict__ 
       for (++tt; tt < D.nterms; ++tt) { T = terms[D.term0 + tt]; if (T.k > 0) { next = true; break; } }
     }
     if (next) gemm_fetch(T, k0, row0, col0, D.m, D.n, ra, rb);
+    // FP64 tensor cores: mma.sync m8n8k4 (DMMA).  Warp w owns the 8x8 output
+    // sub-tiles (si, sj0) and (si, sj0 + 1) of the 32x32 tile; a complex product
+    // is four real products, Cr += Ar Br + (-Ai) Bi and Ci += Ar Bi + Ai Br.
+    // Fragments (PTX ISA, mma.m8n8k4 .f64): A row = lane/4, col = lane%4;
+    // B row = lane%4, col = lane/4; C row = lane/4, cols 2(lane%4) + {0, 1}.
 #pragma unroll
-    for (int kk = 0; kk < TK; ++kk) {
-      const double2 a0 = As[kk][ty], a1 = As[kk][ty + 16];
-      const double2 b0 = Bs[kk][tx], b1 = Bs[kk][tx + 16];
-      acc[0][0] = cfma(a0, b0, acc[0][0]);
-      acc[0][1] = cfma(a0, b1, acc[0][1]);
-      acc[1][0] = cfma(a1, b0, acc[1][0]);
-      acc[1][1] = cfma(a1, b1, acc[1][1]);
+    for (int k4 = 0; k4 < TK; k4 += 4) {
+      const double2 a = As[k4 + (lane & 3)][si * 8 + (lane >> 2)];
+      const double ar = a.x, ai = a.y, nai = -a.y;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const double2 b = Bs[k4 + (lane & 3)][(sj0 + q) * 8 + (lane >> 2)];
+        dmma884(cr[q], ar, b.x);
+        dmma884(cr[q], nai, b.y);
+        dmma884(ci[q], ar, b.y);
+        dmma884(ci[q], ai, b.x);
+      }
     }
     __syncthreads();
     have = next;
   }
   const bool zero_beta = D.beta.x == 0.0 && D.beta.y == 0.0;
-  for (int a = 0; a < 2; ++a)
-    for (int b = 0; b < 2; ++b) {
-      int gi = row0 + ty + 16 * a, gj = col0 + tx + 16 * b;
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int gi = row0 + si * 8 + (lane >> 2), gj = col0 + (sj0 + q) * 8 + 2 * (lane & 3) + h;
       if (gi < D.m && gj < D.n) {
         double2* c = D.C + gi + (size_t)gj * D.ldc;
-        double2 v = cmul(D.alpha, acc[a][b]);
+        double2 v = cmul(D.alpha, make_double2(cr[q][h], ci[q][h]));
         if (!zero_beta) v = cadd(v, cmul(D.beta, *c));
         *c = v;
       }

@@ -4,6 +4,8 @@
 // (LS/LS_Assembly.hpp:808-890, 1074-1087: Morton order, children 0 BL, 1 BR,
 // 2 TR, 3 TL; leaf nodes r * cheb + centre, local index y*n + x) and the
 // contrast / right-hand side functions of LS/LS_functions.hpp:1-120.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace {
@@ -160,5 +162,117 @@ int aifmm_launch_rhs_plane_wave(const double2* pts, const double* q, double kapp
   long blocks = (tot + 255) / 256;
   if (blocks > 148 * 32) blocks = 148 * 32;
   rhs_kernel<<<(int)blocks, 256, 0, s>>>(pts, q, kappa, N, nrhs, theta, b);
+  return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- error norms
+// find_error (FMM2DTree_find_error.hpp:2534-2581): ||x - x_true||^2 and
+// ||x_true||^2 over an n x nrhs block with column strides ldx / ldt.  Each of a
+// fixed number of CTAs sums a fixed slice in a fixed order, and one CTA adds
+// the slices in order, so the result does not depend on timing.
+namespace {
+constexpr int kErrCtas = 148, kErrThreads = 256;
+
+__device__ double block_sum_err(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  v = 0.0;
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  __syncthreads();
+  return v;
+}
+
+__global__ void __launch_bounds__(kErrThreads) err_partial_kernel(const double2* __restrict__ x, long ldx,
+                                                                  const double2* __restrict__ t, long ldt, long n,
+                                                                  int nrhs, double* part) {
+  __shared__ double sh[kErrThreads / 32];
+  const long tot = n * nrhs;
+  double se = 0.0, st = 0.0;
+  for (long e = blockIdx.x * (long)kErrThreads + threadIdx.x; e < tot; e += (long)kErrCtas * kErrThreads) {
+    const long i = e % n, c = e / n;
+    const double2 a = x[i + c * ldx], b = t[i + c * ldt];
+    const double dr = a.x - b.x, di = a.y - b.y;
+    se += dr * dr + di * di;
+    st += b.x * b.x + b.y * b.y;
+  }
+  se = block_sum_err(se, sh);
+  st = block_sum_err(st, sh);
+  if (threadIdx.x == 0) { part[2 * blockIdx.x] = se; part[2 * blockIdx.x + 1] = st; }
+}
+
+__global__ void err_final_kernel(const double* __restrict__ part, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double se = 0.0, st = 0.0;
+    for (int b = 0; b < kErrCtas; ++b) { se += part[2 * b]; st += part[2 * b + 1]; }
+    out[0] = se;
+    out[1] = st;
+  }
+}
+}  // namespace
+
+size_t aifmm_error_norms_scratch_bytes() { return sizeof(double) * 2 * kErrCtas; }
+
+int aifmm_launch_error_norms(const double2* x, long ldx, const double2* t, long ldt, long n, int nrhs, double* part,
+                             double* out2, cudaStream_t s) {
+  err_partial_kernel<<<kErrCtas, kErrThreads, 0, s>>>(x, ldx, t, ldt, n, nrhs, part);
+  err_final_kernel<<<1, 32, 0, s>>>(part, out2);
+  return (int)cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- column kernels (GMRES)
+// For nrhs independent Krylov processes run in lockstep: column c of an
+// N x nrhs block (column stride ld) belongs to process c.  One CTA per column
+// sums its products in a fixed order, so results do not depend on timing.
+namespace {
+constexpr int kColThreads = 512;
+
+__global__ void __launch_bounds__(kColThreads) coldot_kernel(const double2* __restrict__ a, long lda,
+                                                             const double2* __restrict__ b, long ldb, long n,
+                                                             double2* out) {
+  __shared__ double sh[kColThreads / 32];
+  const int c = blockIdx.x;
+  const double2* x = a + c * lda;
+  const double2* y = b + c * ldb;
+  double re = 0.0, im = 0.0;
+  for (long i = threadIdx.x; i < n; i += kColThreads) {  // conj(x) y
+    const double2 u = x[i], v = y[i];
+    re += u.x * v.x + u.y * v.y;
+    im += u.x * v.y - u.y * v.x;
+  }
+  re = block_sum_err(re, sh);
+  im = block_sum_err(im, sh);
+  if (threadIdx.x == 0) out[c] = make_double2(re, im);
+}
+
+// y(:, c) = alpha_c x(:, c) + beta_c y(:, c) with per-column complex coefficients
+__global__ void colaxpby_kernel(const double2* __restrict__ x, long ldx, double2* y, long ldy, long n, int nrhs,
+                                const double2* __restrict__ alpha, const double2* __restrict__ beta) {
+  const long tot = n * nrhs;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < tot; e += (long)gridDim.x * blockDim.x) {
+    const long i = e % n, c = e / n;
+    const double2 a = alpha[c], b = beta[c], u = x[i + c * ldx];
+    double2* v = y + i + c * ldy;
+    const double2 w = *v;
+    *v = make_double2(a.x * u.x - a.y * u.y + b.x * w.x - b.y * w.y, a.x * u.y + a.y * u.x + b.x * w.y + b.y * w.x);
+  }
+}
+}  // namespace
+
+int aifmm_launch_coldot(const double2* a, long lda, const double2* b, long ldb, long n, int nrhs, double2* out,
+                        cudaStream_t s) {
+  coldot_kernel<<<nrhs, kColThreads, 0, s>>>(a, lda, b, ldb, n, out);
+  return (int)cudaGetLastError();
+}
+
+int aifmm_launch_colaxpby(const double2* x, long ldx, double2* y, long ldy, long n, int nrhs, const double2* alpha,
+                          const double2* beta, cudaStream_t s) {
+  const long tot = n * nrhs;
+  const int blocks = (int)std::min<long>((tot + 255) / 256, 148L * 16);
+  colaxpby_kernel<<<blocks, 256, 0, s>>>(x, ldx, y, ldy, n, nrhs, alpha, beta);
   return (int)cudaGetLastError();
 }

@@ -39,6 +39,13 @@ int aifmm_launch_rhs_plane_wave(const double2* pts, const double* q, double kapp
 int aifmm_launch_incident_field(const double2* pts, double kappa, int N, int nrhs, const double* theta, double2* u,
                                 cudaStream_t s);
 int aifmm_launch_gather_segments(const int* src, const int4* segs, long nseg, int* dst, cudaStream_t s);
+size_t aifmm_error_norms_scratch_bytes();
+int aifmm_launch_error_norms(const double2* x, long ldx, const double2* t, long ldt, long n, int nrhs, double* part,
+                             double* out2, cudaStream_t s);
+int aifmm_launch_coldot(const double2* a, long lda, const double2* b, long ldb, long n, int nrhs, double2* out,
+                        cudaStream_t s);
+int aifmm_launch_colaxpby(const double2* x, long ldx, double2* y, long ldy, long n, int nrhs, const double2* alpha,
+                          const double2* beta, cudaStream_t s);
 
 namespace {
 
@@ -127,21 +134,36 @@ class Pool {
   size_t left_ = 0;
 };
 
-// Bump allocator for per-step scratch (reset when a box step ends).
+// Bump allocator for per-step scratch (reset when a box step ends).  It starts
+// with one chunk sized for the problem and chains further chunks when a step
+// needs more; chunks are kept and reused after every reset.
 class Arena {
  public:
-  void init(size_t bytes) { CK(cudaMalloc(&base_, bytes)); cap_ = bytes; off_ = 0; }
-  ~Arena() { if (base_) cudaFree(base_); }
+  void init(size_t bytes) { add_chunk(bytes); }
+  ~Arena() { for (auto& c : chunks_) cudaFree(c.first); }
   void* get(size_t bytes) {
     size_t b = (bytes + 255) & ~size_t(255);
-    if (off_ + b > cap_) throw Fail(AIFMM_ERR_NOMEM, "scratch arena exhausted");
-    void* p = base_ + off_;
+    while (cur_ < chunks_.size() && off_ + b > chunks_[cur_].second) { ++cur_; off_ = 0; }
+    if (cur_ == chunks_.size()) { add_chunk(std::max(b, chunks_.empty() ? b : chunks_.back().second)); off_ = 0; }
+    void* p = chunks_[cur_].first + off_;
     off_ += b;
     return p;
   }
-  void reset() { off_ = 0; }
-  char* base_ = nullptr;
-  size_t cap_ = 0, off_ = 0;
+  void reset() { cur_ = 0; off_ = 0; }
+  size_t capacity() const {
+    size_t s = 0;
+    for (auto& c : chunks_) s += c.second;
+    return s;
+  }
+
+ private:
+  void add_chunk(size_t bytes) {
+    char* p = nullptr;
+    CK(cudaMalloc(&p, bytes));
+    chunks_.push_back({p, bytes});
+  }
+  std::vector<std::pair<char*, size_t>> chunks_;
+  size_t cur_ = 0, off_ = 0;
 };
 
 // Pinned host + device ring for launch descriptors.  When the ring wraps, the
@@ -224,6 +246,11 @@ class GrowBuf {
     return p_;
   }
   size_t capacity() const { return cap_; }
+  void release() {  // the caller has synchronised every stream that used the buffer
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    cap_ = 0;
+  }
 
  private:
   void* p_ = nullptr;
@@ -253,9 +280,15 @@ struct Box {
   int NumM = 0, NumL = 0;
   std::vector<int> in_check, in_charge, out_check, out_charge;
   int rank_in = 0, rank_out = 0;
-  Blk Ac, Ar, L2P, P2M, L2P_f, L2M_f;
+  Blk Ac, Ar, L2P, P2M, L2M_f;
+  // Lf[n]: the fill-in L2P_f of neighbour nb[n] formed when this box was
+  // eliminated (F:1962-1972); the z-phase and every later solve read it
+  Blk Lf[8];
   std::map<int, Blk> M2L, P2P, M2P, P2L, P2M_f, M2M_f;
-  Blk prhs, mrhs, lrhs, particles, multipoles, locals;
+  // per-solve state: sr the box's particle right-hand side once its
+  // smaller-index neighbours are eliminated, sxb = QRx^-1 sr, sy = QRz^-1 (-P2M sxb),
+  // smr the multipole right-hand side handed to the parent level
+  Blk sr, sxb, sy, smr, particles, multipoles, locals;
   QRF qx, qz;
 };
 
@@ -331,7 +364,8 @@ struct aifmm_problem {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string err;
   int rank = 0, N = 0, nleaf = 0, depth = 0, nb = 0;
-  double tol = 0;
+  double tol = 0;         // ACA (assembly) tolerance, 10^-tol_pow
+  double tol_factor = 0;  // recompression tolerance of the factorisation (tol unless set)
   // device geometry and tables
   double2 *d_pts = nullptr, *d_leafc = nullptr, *d_M = nullptr, *d_near = nullptr;
   double* d_q = nullptr;
@@ -675,6 +709,12 @@ struct aifmm_problem {
   // interpolative operators, M2L/P2P block entries (launch to completion)
   double st_asm_lists_ms = 0, st_asm_aca_ms = 0, st_asm_lu_ms = 0, st_asm_blocks_ms = 0, st_asm_aca_gpu_ms = 0;
   long st_syncs = 0, st_compress = 0, st_apicalls = 0;
+  // device -> host read on the handle's stream (never the legacy default stream,
+  // which would order this handle against other handles' work)
+  void d2h(void* dst, const void* src, size_t bytes) {
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
   void sync() {
     auto t0 = std::chrono::steady_clock::now();
     CK(cudaStreamSynchronize(st));
@@ -706,8 +746,10 @@ struct aifmm_problem {
     N = nleaf * rank;
     nb = d.degree * (d.degree + 1) / 2;
     tol = std::pow(10, -1.0 * d.tol_pow);
+    tol_factor = tol;
     stage.init(size_t(64) << 20, st, st2);
-    scratch.init(size_t(2) << 30);
+    // per-step scratch: ~1 KB per unknown (2 GB at 589,824 unknowns), at least 64 MB
+    scratch.init(std::min(size_t(2) << 30, std::max(size_t(64) << 20, (size_t)N * 3600)));
     CK(cudaMalloc(&d_pts, sizeof(double2) * N));
     CK(cudaMalloc(&d_q, sizeof(double) * N));
     CK(cudaMalloc(&d_leafc, sizeof(double2) * nleaf));
@@ -1176,7 +1218,7 @@ struct aifmm_problem {
   // blocks towards its neighbours.  So the factorisation of P2P[k][k] and its
   // solves with those blocks run on the second stream, overlapping the
   // recompressions and their synchronisations on the main stream.
-  struct SideX { bool on = false; Blk Xb, W[8]; };
+  struct SideX { bool on = false; Blk W[8]; };
   SideX sx;
   void eliminate_x_side(int j, int k) {
     sx = SideX();
@@ -1190,8 +1232,6 @@ struct aifmm_problem {
     qr_prepare(B.qx, Pkk, 0.0, true);  // factored in place; P2P[k][k] is not read again
     flush_qr();
     const int m = Pkk.c;
-    sx.Xb = scr(m, nrhs);
-    solve(B.qx, B.prhs, sx.Xb, C1);
     for (int pI = 0; pI < 8; ++pI) {
       const int pp = B.nb[pI];
       if (pp == -1) continue;
@@ -1209,18 +1249,15 @@ struct aifmm_problem {
     Blk& Pkk = B.P2P[k];
     if (Pkk.size() != 0) {
       const int m = Pkk.c;
-      Blk XL = scr(m, B.L2P.c), Xb, W[8];
+      Blk XL = scr(m, B.L2P.c), W[8];
       if (sx.on) {
         CK(cudaStreamWaitEvent(st, ev_join, 0));
-        Xb = sx.Xb;
         for (int q = 0; q < 8; ++q) W[q] = sx.W[q];
         solve(B.qx, B.L2P, XL, C1);
       } else {
         qr_prepare(B.qx, Pkk, 0.0, true);
         flush_qr();
-        Xb = scr(m, nrhs);
         solve(B.qx, B.L2P, XL, C1);
-        solve(B.qx, B.prhs, Xb, C1);
         for (int pI = 0; pI < 8; ++pI) {
           const int pp = B.nb[pI];
           if (pp == -1) continue;
@@ -1239,7 +1276,6 @@ struct aifmm_problem {
         gemm(t, B.P2M, 0, W[n], 0, CM1, C0);
         if (!T[j][nn].elim) assign(B.P2M_f[nn], t); else assign(B.M2M_f[nn], t);
       }
-      { Blk t = newblk(B.P2M.r, nrhs); gemm(t, B.P2M, 0, Xb, 0, CM1, C0); assign(B.lrhs, t); }
       // box k's own products first: the z-phase factorisation and solves need only
       // them, and run on the second stream while the fill-ins of the neighbours'
       // blocks below are computed
@@ -1250,7 +1286,7 @@ struct aifmm_problem {
         if (nn == -1) continue;
         Box& Nn = T[j][nn];
         const Blk Xnk = X_of(Nn, Nn.elim, k);
-        { Blk t = newblk(Xnk.r, XL.c); gemm(t, Xnk, 0, XL, 0, CM1, C0); assign(Nn.L2P_f, t); }
+        { Blk t = newblk(Xnk.r, XL.c); gemm(t, Xnk, 0, XL, 0, CM1, C0); assign(B.Lf[n], t); }
         for (int pI = 0; pI < 8; ++pI) {
           const int pp = B.nb[pI];
           if (pp == -1) continue;
@@ -1269,7 +1305,6 @@ struct aifmm_problem {
           }
           if (kind >= 0) record_cand(kind, nn, pp, *tgt);
         }
-        gemm(Nn.elim ? Nn.mrhs : Nn.prhs, Xnk, 0, Xb, 0, CM1, C1);
       }
       flush_gemm();
       flush_norms(0);
@@ -1283,12 +1318,11 @@ struct aifmm_problem {
         if (!T[j][nn].elim) { Blk t = newblk(B.P2M.r, B.P2P[nn].c); zero(t); assign(B.P2M_f[nn], t); }
         else { Blk t = newblk(B.P2M.r, B.M2P[nn].c); zero(t); assign(B.M2M_f[nn], t); }
       }
-      { Blk t = newblk(B.P2M.r, nrhs); zero(t); assign(B.lrhs, t); }
       for (int n = 0; n < 8; ++n) {
         const int nn = B.nb[n];
         if (nn == -1) continue;
         Box& Nn = T[j][nn];
-        { Blk t = newblk(X_of(Nn, Nn.elim, k).r, B.L2P.c); zero(t); assign(Nn.L2P_f, t); }
+        { Blk t = newblk(X_of(Nn, Nn.elim, k).r, B.L2P.c); zero(t); assign(B.Lf[n], t); }
         for (int pI = 0; pI < 8; ++pI) {
           const int pp = B.nb[pI];
           if (pp == -1) continue;
@@ -1330,7 +1364,6 @@ struct aifmm_problem {
       else { Blk t = newblk(nl, B.M2M_f[nn].c); solve(B.qz, B.M2M_f[nn], t, C1); assign(B.M2L[nn], t); }
       // well-separated test of (k, nn) is false for a neighbour: nothing is queued here
     }
-    { Blk t = newblk(nl, nrhs); solve(B.qz, B.lrhs, t, C1); assign(B.mrhs, t); }
     flush_solve();
   }
   void eliminate_z_side(int j, int k) {
@@ -1351,12 +1384,12 @@ struct aifmm_problem {
       if (sz_on) CK(cudaStreamWaitEvent(st, ev_join, 0));
       else eliminate_z_qr_solves(j, k);
       sz_on = false;
-      const Blk Yneg = B.M2L[k], Yrhs = B.mrhs;
+      const Blk Yneg = B.M2L[k];
       for (int n = 0; n < 8; ++n) {
         const int nn = B.nb[n];
         if (nn == -1) continue;
         Box& Nn = T[j][nn];
-        const Blk Lf = Nn.L2P_f;
+        const Blk Lf = B.Lf[n];
         {  // F:2348-2372
           Blk& tgt = Nn.elim ? Nn.M2L[k] : Nn.M2P[k];
           if (tgt.size() == 0) { Blk t = newblk(Lf.r, Yneg.c); gemm(t, Lf, 0, Yneg, 0, CM1, C0); assign(tgt, t); }
@@ -1374,7 +1407,6 @@ struct aifmm_problem {
           gemm(*tgt, Lf, 0, Z, 0, CM1, C1);
           if (kind >= 0) record_cand(kind, nn, pp, *tgt);
         }
-        gemm(Nn.elim ? Nn.mrhs : Nn.prhs, Lf, 0, Yrhs, 0, CM1, C1);
       }
       flush_gemm();
       flush_norms(1);
@@ -1386,13 +1418,12 @@ struct aifmm_problem {
         if (!T[j][nn].elim) { Blk t = newblk(0, B.P2M_f[nn].c); assign(B.P2L[nn], t); }
         else { Blk t = newblk(0, B.M2M_f[nn].c); assign(B.M2L[nn], t); }
       }
-      { Blk t = newblk(0, nrhs); assign(B.mrhs, t); }
       for (int n = 0; n < 8; ++n) {
         const int nn = B.nb[n];
         if (nn == -1) continue;
         Box& Nn = T[j][nn];
         Blk& tgt = Nn.elim ? Nn.M2L[k] : Nn.M2P[k];
-        if (tgt.size() == 0) { Blk t = newblk(Nn.L2P_f.r, B.NumM); zero(t); assign(tgt, t); }
+        if (tgt.size() == 0) { Blk t = newblk(B.Lf[n].r, B.NumM); zero(t); assign(tgt, t); }
         for (int pI = 0; pI < 8; ++pI) {
           const int pp = B.nb[pI];
           if (pp == -1) continue;
@@ -1446,7 +1477,7 @@ struct aifmm_problem {
       J.Pkb = Pkb.p; J.ldP = Pkb.ld;
       J.P2M = Bb.P2M.p; J.ldM = Bb.P2M.ld;
       J.M2L = m2l.p; J.ldT = m2l.ld;
-      J.m = m; J.rK = rK; J.c = c; J.rb = rb; J.tol = tol;
+      J.m = m; J.rK = rK; J.c = c; J.rb = rb; J.tol = tol_factor;
       J.nL = out[s]->nL.p; J.nPt = out[s]->nPt.p;
       J.M2Lo = out[s]->M2L.p; J.ldO = out[s]->M2L.ld;
       J.ranks = ranks + 2 * s;
@@ -1467,7 +1498,7 @@ struct aifmm_problem {
     KL(aifmm_launch_compress_p2p(dj, 2, smem, st));
     sync();
     int rk[4];
-    CK(cudaMemcpy(rk, ranks, sizeof rk, cudaMemcpyDeviceToHost));
+    d2h(rk, ranks, sizeof rk);
     for (int s = 0; s < 2; ++s) {
       const int rc = rk[2 * s], rr = rk[2 * s + 1];
       if (rc < 0 || rc > rcmax[s] || rr < 0 || rr > rrmax[s]) throw Fail(AIFMM_ERR_NUMERIC, "compress_P2P: rank out of range");
@@ -1495,12 +1526,12 @@ struct aifmm_problem {
       copy(Blk{Acol[s].p + (size_t)K.L2P.c * Acol[s].ld, Pkb.r, Pkb.c, Acol[s].ld}, Pkb);
     }
     flush_geam();
-    for (int s = 0; s < 2; ++s) qr_prepare(qc[s], Acol[s], tol, false);
+    for (int s = 0; s < 2; ++s) qr_prepare(qc[s], Acol[s], tol_factor, false);
     flush_qr();
     sync();
     for (int s = 0; s < 2; ++s) {
       int info[2];
-      CK(cudaMemcpy(info, qc[s].info, sizeof info, cudaMemcpyDeviceToHost));
+      d2h(info, qc[s].info, sizeof info);
       rc[s] = info[1];
     }
     for (int s = 0; s < 2; ++s) {
@@ -1525,12 +1556,12 @@ struct aifmm_problem {
       geam(Blk{Arow[s].p + (size_t)rb * Arow[s].ld, mb, rc[s], Arow[s].ld}, Rk_prime[s], 1, C1, C0);
     }
     flush_geam();
-    for (int s = 0; s < 2; ++s) qr_prepare(qw[s], Arow[s], tol, false);
+    for (int s = 0; s < 2; ++s) qr_prepare(qw[s], Arow[s], tol_factor, false);
     flush_qr();
     sync();
     for (int s = 0; s < 2; ++s) {
       int info[2];
-      CK(cudaMemcpy(info, qw[s].info, sizeof info, cudaMemcpyDeviceToHost));
+      d2h(info, qw[s].info, sizeof info);
       rr[s] = info[1];
     }
     for (int s = 0; s < 2; ++s) {
@@ -1712,13 +1743,13 @@ struct aifmm_problem {
     geam(Blk{Arow.p + (size_t)rk * Arow.ld, mk, Lbk.r, Arow.ld}, Lbk, 1, C1, C0);
     flush_geam();
     QRF qc, qw;
-    qr_prepare(qc, Acol, tol, false);
-    qr_prepare(qw, Arow, tol, false);
+    qr_prepare(qc, Acol, tol_factor, false);
+    qr_prepare(qw, Arow, tol_factor, false);
     flush_qr();
     sync();
     int ic[2], iw[2];
-    CK(cudaMemcpy(ic, qc.info, sizeof ic, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(iw, qw.info, sizeof iw, cudaMemcpyDeviceToHost));
+    d2h(ic, qc.info, sizeof ic);
+    d2h(iw, qw.info, sizeof iw);
     const int rc = ic[1], rr = iw[1];
     Blk nLk = newblk(Acol.r, rc), nPtk = newblk(Arow.r, rr);
     formq(qc, nLk);
@@ -1796,16 +1827,6 @@ struct aifmm_problem {
       };
       for (int n = 0; n < 8; ++n) if (B.nb[n] != -1) { Blk P = mosaic(B.nb[n]); assign(B.P2P[B.nb[n]], P); }
       { Blk P = mosaic(k); assign(B.P2P[k], P); }
-      int len = 0;
-      for (int c = 0; c < 4; ++c) len += T[j + 1][4 * k + c].NumL;
-      Blk r = newblk(len, nrhs);
-      int o = 0;
-      for (int c = 0; c < 4; ++c) {
-        const Blk& m = T[j + 1][4 * k + c].mrhs;
-        copy(Blk{r.p + o, m.r, nrhs, r.ld}, m);
-        o += m.r;
-      }
-      assign(B.prhs, r);
       if ((int)ged.size() > 20000) flush_geam();
     }
     flush_geam();
@@ -1892,7 +1913,7 @@ struct aifmm_problem {
       sync();
       clear_cands();  // pending pairs never cross a level
     }
-    solve_base(2);
+    factor_base(2);
   }
 
   void end_step() {
@@ -1902,37 +1923,155 @@ struct aifmm_problem {
     pool.commit_frees();
   }
 
-  void solve_base(int j) {  // F:2453-2485
+  // F:2453-2485, factorisation half: the dense level-2 system (each box's
+  // locals against every box's multipoles through the level's M2L blocks) is
+  // factored once and kept for every solve.
+  Blk base_A;
+  QRF base_qr;
+  int base_NL = 0, base_NM = 0;
+  void factor_base(int j) {
+    drop(base_A);
+    drop_qrf(base_qr);
     int NM = 0, NL = 0;
     for (int k = 0; k < nBoxes[j]; ++k) { NM += T[j][k].NumM; NL += T[j][k].NumL; }
-    if (NL == 0 || NM == 0) {
-      for (int k = 0; k < nBoxes[j]; ++k) { Blk t = newblk(T[j][k].NumM, nrhs); zero(t); assign(T[j][k].multipoles, t); }
-      return;
-    }
-    Blk A = scr(NL, NM), b = scr(NL, nrhs);
-    zero(A);
+    base_NL = NL;
+    base_NM = NM;
+    if (NL == 0 || NM == 0) { end_step(); return; }
+    base_A = newblk(NL, NM);
+    zero(base_A);
     int ri = 0;
     for (int r = 0; r < nBoxes[j]; ++r) {
       Box& R = T[j][r];
       int si = 0;
-      for (int s = 0; s < nBoxes[j]; ++s) {
-        const int nc = T[j][s].NumM;
+      for (int s_ = 0; s_ < nBoxes[j]; ++s_) {
+        const int nc = T[j][s_].NumM;
         if (R.NumL > 0 && nc > 0) {
-          const Blk& m = R.M2L[s];
+          const Blk& m = R.M2L[s_];
           if (m.r != R.NumL || m.c != nc) throw Fail(AIFMM_ERR_NUMERIC, "base level: M2L block has the wrong shape");
-          copy(Blk{A.p + ri + (size_t)si * A.ld, m.r, m.c, A.ld}, m);
+          copy(Blk{base_A.p + ri + (size_t)si * base_A.ld, m.r, m.c, base_A.ld}, m);
         }
         si += nc;
       }
-      copy(Blk{b.p + ri, R.NumL, nrhs, b.ld}, R.mrhs);
       ri += R.NumL;
     }
     flush_geam();
-    QRF f;
-    qr_prepare(f, A, 0.0, false);
+    qr_prepare(base_qr, base_A, 0.0, true);
     flush_qr();
-    Blk mp = scr(NM, nrhs);
-    solve(f, b, mp, C1);
+    end_step();
+  }
+
+  // ---- solve with kept factors
+  //
+  // The reference carries the right-hand side through the elimination
+  // (F:1968, 1997-2001, 2252, 2289-2293) and solves the base level (F:2453-2485)
+  // and the back substitution (F:2487-2532) with it.  Eliminating box s
+  // subtracts X[t][s] QRx_s^-1 r_s (eliminate_x) and L2P_f[t] y_s (eliminate_z)
+  // from the right-hand side of every neighbour t: the particle one while t is
+  // not eliminated (t > s), the multipole one after (t < s).  Every block in
+  // these products is frozen once s is eliminated, except L2P_f, which the
+  // elimination keeps per box and neighbour slot (Lf).  Gathered per receiving
+  // box k, with rhs_k the leaf right-hand side or the children's multipole ones:
+  //   sr_k  = rhs_k - sum_{nn < k} (P2P[k][nn] sxb_nn + Lf_{k,nn} sy_nn)
+  //   sxb_k = QRx_k^-1 sr_k,  sy_k = QRz_k^-1 (-P2M_k sxb_k)
+  //   smr_k = sy_k  - sum_{nn > k} (P2L[k][nn] sxb_nn + Lf_{k,nn} sy_nn)
+  // where Lf_{k,nn} is the Lf of box nn at the slot that faces k.  sr_k needs
+  // only smaller-index neighbours, so the forward sweep runs in waves like the
+  // back substitution; smr needs the whole level and is one batch after it.
+  std::vector<std::vector<std::vector<int>>> fwd_waves, bwd_waves;
+  // wave(k) = 1 + the largest wave among k's neighbours that come before k in
+  // the sweep (smaller index forward, larger index backward): the boxes of a
+  // wave are pairwise non-adjacent and read only what earlier waves wrote.
+  std::vector<std::vector<int>> level_waves(int j, bool forward) const {
+    const int nbx = nBoxes[j];
+    std::vector<int> wave(nbx, 0);
+    int nw = 0;
+    for (int t = 0; t < nbx; ++t) {
+      const int k = forward ? t : nbx - 1 - t;
+      int w = 0;
+      for (int n = 0; n < 8; ++n) {
+        const int nn = T[j][k].nb[n];
+        if (nn != -1 && (forward ? nn < k : nn > k)) w = std::max(w, wave[nn] + 1);
+      }
+      wave[k] = w;
+      nw = std::max(nw, w + 1);
+    }
+    std::vector<std::vector<int>> waves(nw);
+    for (int t = 0; t < nbx; ++t) {
+      const int k = forward ? t : nbx - 1 - t;
+      waves[wave[k]].push_back(k);
+    }
+    return waves;
+  }
+  const Blk& lf_towards(int j, int k, int n) const {  // Lf of neighbour nb[n] at the slot facing k
+    const Box& Nn = T[j][T[j][k].nb[n]];
+    return Nn.Lf[(n + 4) & 7];
+  }
+  void forward_level(int j) {
+    for (const auto& ks : fwd_waves[j]) {
+      for (int k : ks) {
+        Box& B = T[j][k];
+        std::vector<std::pair<Blk, Blk>> terms;
+        for (int n = 0; n < 8; ++n) {
+          const int nn = B.nb[n];
+          if (nn == -1 || nn > k) continue;
+          terms.push_back({B.P2P[nn], T[j][nn].sxb});
+          terms.push_back({lf_towards(j, k, n), T[j][nn].sy});
+        }
+        gemm_sum(B.sr, terms, CM1, C1);
+      }
+      flush_gemm();
+      for (int k : ks) {
+        Box& B = T[j][k];
+        if (B.P2P[k].size() != 0) solve(B.qx, B.sr, B.sxb, C1);
+      }
+      flush_solve();
+      std::vector<Blk> lr(ks.size());
+      for (size_t q = 0; q < ks.size(); ++q) {
+        Box& B = T[j][ks[q]];
+        if (B.L2M_f.size() == 0) continue;
+        lr[q] = scr(B.P2M.r, nrhs);
+        gemm(lr[q], B.P2M, 0, B.sxb, 0, CM1, C0);
+      }
+      flush_gemm();
+      for (size_t q = 0; q < ks.size(); ++q) {
+        Box& B = T[j][ks[q]];
+        if (B.L2M_f.size() != 0) solve(B.qz, lr[q], B.sy, C1);
+      }
+      flush_solve();
+      end_step();
+    }
+    for (int k = 0; k < nBoxes[j]; ++k) copy(T[j][k].smr, T[j][k].sy);
+    flush_geam();
+    for (int k = 0; k < nBoxes[j]; ++k) {
+      Box& B = T[j][k];
+      std::vector<std::pair<Blk, Blk>> terms;
+      for (int n = 0; n < 8; ++n) {
+        const int nn = B.nb[n];
+        if (nn == -1 || nn < k) continue;
+        terms.push_back({B.P2L[nn], T[j][nn].sxb});
+        terms.push_back({lf_towards(j, k, n), T[j][nn].sy});
+      }
+      gemm_sum(B.smr, terms, CM1, C1);
+      if ((int)gd.size() > 20000) flush_gemm();
+    }
+    flush_gemm();
+    end_step();
+  }
+  void solve_base_rhs(int j) {  // F:2453-2485, solve half
+    if (base_NL == 0 || base_NM == 0) {
+      for (int k = 0; k < nBoxes[j]; ++k) { Blk t = newblk(T[j][k].NumM, nrhs); zero(t); assign(T[j][k].multipoles, t); }
+      return;
+    }
+    Blk b = scr(base_NL, nrhs);
+    int ri = 0;
+    for (int r = 0; r < nBoxes[j]; ++r) {
+      Box& R = T[j][r];
+      copy(Blk{b.p + ri, R.NumL, nrhs, b.ld}, R.smr);
+      ri += R.NumL;
+    }
+    flush_geam();
+    Blk mp = scr(base_NM, nrhs);
+    solve(base_qr, b, mp, C1);
     flush_solve();
     int o = 0;
     for (int k = 0; k < nBoxes[j]; ++k) {
@@ -1944,35 +2083,12 @@ struct aifmm_problem {
     flush_geam();
     end_step();
   }
-
   // F:2487-2532 (the factorisations of the elimination are reused).  The
   // reference visits the boxes of a level in decreasing order; box k reads the
   // particles of its neighbours with a larger index (already solved) and the
-  // multipoles of the others (known from the level above).  A box therefore only
-  // waits for its larger-index neighbours: with wave(k) = 1 + max wave of those
-  // neighbours, the boxes of one wave are pairwise non-adjacent, everything they
-  // read was written by earlier waves, and each box computes exactly what the
-  // sequential order computes.  Every phase below is one batched launch per wave.
-  void back_substitution_phase() {
-    for (int j = 2; j <= depth; ++j) {
-      const int nbx = nBoxes[j];
-      std::vector<int> wave(nbx, 0);
-      int nw = 0;
-      for (int k = nbx - 1; k >= 0; --k) {
-        int w = 0;
-        for (int n = 0; n < 8; ++n) {
-          const int nn = T[j][k].nb[n];
-          if (nn > k) w = std::max(w, wave[nn] + 1);
-        }
-        wave[k] = w;
-        nw = std::max(nw, w + 1);
-      }
-      std::vector<std::vector<int>> waves(nw);
-      for (int k = nbx - 1; k >= 0; --k) waves[wave[k]].push_back(k);
-      for (const auto& ks : waves) back_substitute_wave(j, ks);
-    }
-  }
-  void back_substitute_wave(int j, const std::vector<int>& ks) {
+  // multipoles of the others (known from the level above).  The backward waves
+  // give each box exactly what the sequential order gives it.
+  void backward_wave(int j, const std::vector<int>& ks) {
     struct Work { Blk rhs1, t, rhs2, v; };
     std::vector<Work> wk(ks.size());
     std::vector<int> act;  // boxes with unknowns at this level
@@ -1981,16 +2097,17 @@ struct aifmm_problem {
     for (int q : act) {
       Box& B = T[j][ks[q]];
       wk[q].rhs1 = scr(B.P2P[ks[q]].r, nrhs);
-      copy(wk[q].rhs1, B.prhs);
+      copy(wk[q].rhs1, B.sr);
     }
     flush_geam();
     for (int q : act) {
-      Box& B = T[j][ks[q]];
+      const int k = ks[q];
+      Box& B = T[j][k];
       std::vector<std::pair<Blk, Blk>> terms;
       for (int n = 0; n < 8; ++n) {
         const int nn = B.nb[n];
         if (nn == -1) continue;
-        if (!T[j][nn].elim) terms.push_back({B.P2P[nn], T[j][nn].particles});
+        if (nn > k) terms.push_back({B.P2P[nn], T[j][nn].particles});
         else terms.push_back({B.M2P[nn], T[j][nn].multipoles});
       }
       gemm_sum(wk[q].rhs1, terms, CM1, C1);
@@ -2035,7 +2152,6 @@ struct aifmm_problem {
       const int k = ks[q];
       Box& B = T[j][k];
       if (B.P2P[k].size() == 0) { Blk px = newblk(0, nrhs); assign(B.particles, px); }
-      B.elim = false;
       if (j != depth) {
         int o = 0;
         for (int c = 0; c < 4; ++c) {
@@ -2048,18 +2164,28 @@ struct aifmm_problem {
     }
     end_step();
   }
+  void release_solve_state() {
+    for (auto& lv : T)
+      for (auto& B : lv) {
+        drop(B.sr); drop(B.sxb); drop(B.sy); drop(B.smr);
+        drop(B.particles); drop(B.locals); drop(B.multipoles);
+      }
+  }
 
   void release_level_data() {
     for (auto& lv : T)
       for (auto& B : lv) {
         auto dm = [&](std::map<int, Blk>& m) { for (auto& kv : m) drop(kv.second); m.clear(); };
         dm(B.M2L); dm(B.P2P); dm(B.M2P); dm(B.P2L); dm(B.P2M_f); dm(B.M2M_f);
-        drop(B.L2P_f); drop(B.L2M_f); drop(B.prhs); drop(B.mrhs); drop(B.lrhs); drop(B.locals);
-        drop(B.particles);
-        drop(B.multipoles);
+        for (auto& l : B.Lf) drop(l);
+        drop(B.L2M_f);
         drop_qrf(B.qx); drop_qrf(B.qz);
         B.elim = false;
       }
+    release_solve_state();
+    drop(base_A);
+    drop_qrf(base_qr);
+    factored = false;
   }
   // Everything a tree holds, before the tree is rebuilt: the elimination's blocks
   // and factorisations, the bases, the ACA factors and the kept copy of the
@@ -2078,68 +2204,373 @@ struct aifmm_problem {
   }
 
   bool consumed = false;  // the elimination consumed the assembled blocks
-  void factorize_solve(int nrhs_, const double* b, double* x, int flags) {
-    if (!assembled) throw Fail(AIFMM_ERR_STATE, "assemble() must run before factorize_solve()");
+  bool factored = false;  // factors are kept: solve() may run any number of times
+  double ms_factor = 0, ms_solve = 0;
+  long launches_factor = 0, launches_solve = 0;
+  // eliminate_phase_efficient with the base-level factorisation (F:2407-2485),
+  // right-hand side not carried
+  void factorize(int flags) {
+    if (!assembled) throw Fail(AIFMM_ERR_STATE, "assemble() must run before factorize()");
     if (consumed && !have_saved)
-      throw Fail(AIFMM_ERR_STATE, "the assembly was consumed by a previous solve: assemble again, or pass AIFMM_KEEP_ASSEMBLY");
+      throw Fail(AIFMM_ERR_STATE, "the assembly was consumed by a previous factorisation: assemble again, or pass AIFMM_KEEP_ASSEMBLY");
+    auto t0 = std::chrono::steady_clock::now();
+    const long l0 = launches_;
+    // the elimination consumes the assembled blocks; with AIFMM_KEEP_ASSEMBLY a
+    // pristine copy is kept so that the handle can be factored again
+    if ((flags & AIFMM_KEEP_ASSEMBLY) || have_saved) snapshot_restore();
+    release_solve_state();
+    factored = false;
+    consumed = true;
+    st_sync_ms = st_compress_ms = st_elim_ms = st_pending_ms = 0;
+    st_syncs = st_compress = 0;
+    eliminate_phase_efficient();
+    fwd_waves.assign(depth + 1, {});
+    bwd_waves.assign(depth + 1, {});
+    for (int j = 2; j <= depth; ++j) {
+      fwd_waves[j] = level_waves(j, true);
+      bwd_waves[j] = level_waves(j, false);
+      for (int k = 0; k < nBoxes[j]; ++k)
+        for (int n = 0; n < 8; ++n) {
+          const int nn = T[j][k].nb[n];
+          if (nn != -1 && T[j][nn].nb[(n + 4) & 7] != k) throw Fail(AIFMM_ERR_NUMERIC, "neighbour slots not mirrored");
+        }
+    }
+    sync();
+    CK(cudaStreamSynchronize(st2));
+    prof_collect();
+    pool.commit_frees();
+    factored = true;
+    launches_factor = launches_ - l0;
+    ms_factor = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+
+  // b and x: N x nrhs complex, column stride ldb / ldx (>= N), host or device
+  void solve_rhs(int nrhs_, const double* b, long ldb, double* x, long ldx, int flags) {
+    if (!factored) throw Fail(AIFMM_ERR_STATE, "factorize() must run before solve()");
     if (nrhs_ < 1) throw Fail(AIFMM_ERR_ARG, "nrhs must be positive");
+    if (ldb < N || ldx < N) throw Fail(AIFMM_ERR_ARG, "leading dimension smaller than the number of unknowns");
     auto t0 = std::chrono::steady_clock::now();
     const long l0 = launches_;
     nrhs = nrhs_;
-    // the elimination consumes the assembled blocks; with AIFMM_KEEP_ASSEMBLY a
-    // pristine copy is kept so that the handle can be solved again
-    if ((flags & AIFMM_KEEP_ASSEMBLY) || have_saved) snapshot_restore();
-    consumed = true;
+    const bool dev = flags & AIFMM_PTR_DEVICE;
     const size_t bytes = sizeof(double2) * (size_t)N * nrhs;
-    double2* db = nullptr;
-    if (flags & AIFMM_PTR_DEVICE) db = reinterpret_cast<double2*>(const_cast<double*>(b));
-    else {
-      db = static_cast<double2*>(pool.alloc(bytes));
-      CK(cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, st));
+    Tmp tb(this, dev ? 1 : bytes), tx(this, dev ? 1 : bytes);
+    const double2* db = reinterpret_cast<const double2*>(b);
+    long ldd_b = ldb;
+    if (!dev) {
+      CK(cudaMemcpy2DAsync(tb.ptr, sizeof(double2) * N, b, sizeof(double2) * ldb, sizeof(double2) * N, nrhs,
+                           cudaMemcpyHostToDevice, st));
+      db = tb.as<double2>();
+      ldd_b = N;
     }
-    // assign_Leaf_rhs (F:1092-1103)
-    for (int k = 0; k < nBoxes[depth]; ++k) {
-      Box& B = T[depth][k];
-      Blk r = newblk(rank, nrhs);
-      copy(r, Blk{db + (size_t)k * rank, rank, nrhs, N});
-      assign(B.prhs, r);
-      if ((int)ged.size() > 20000) flush_geam();
-    }
+    // per-solve blocks: every box's rhs, sxb, sy, smr
+    release_solve_state();
     for (int j = 2; j <= depth; ++j)
       for (int k = 0; k < nBoxes[j]; ++k) {
         Box& B = T[j][k];
-        Blk m = newblk(B.NumL, nrhs); zero(m); assign(B.mrhs, m);
-        Blk l = newblk(B.NumM, nrhs); zero(l); assign(B.lrhs, l);
+        const int m = B.P2P[k].r;
+        B.sr = newblk(m, nrhs);
+        B.sxb = newblk(B.P2P[k].size() != 0 ? B.P2P[k].c : 0, nrhs);
+        B.sy = newblk(B.L2M_f.size() != 0 ? B.L2M_f.c : 0, nrhs);
+        B.smr = newblk(B.sy.r, nrhs);
       }
+    // assign_Leaf_rhs (F:1092-1103)
+    for (int k = 0; k < nBoxes[depth]; ++k) {
+      Box& B = T[depth][k];
+      copy(B.sr, Blk{const_cast<double2*>(db) + (size_t)k * rank, rank, nrhs, (int)ldd_b});
+      if ((int)ged.size() > 20000) flush_geam();
+    }
     flush_geam();
-    end_step();
-    st_sync_ms = st_compress_ms = st_elim_ms = st_back_ms = st_pending_ms = 0;
-    st_syncs = st_compress = 0;
-    eliminate_phase_efficient();
-    auto tb0 = std::chrono::steady_clock::now();
-    back_substitution_phase();
-    st_back_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb0).count();
+    for (int j = depth; j >= 2; --j) {
+      if (j != depth) {  // the children's multipole right-hand sides (F:1798-1807)
+        for (int k = 0; k < nBoxes[j]; ++k) {
+          Box& B = T[j][k];
+          int o = 0;
+          for (int c = 0; c < 4; ++c) {
+            const Blk& m = T[j + 1][4 * k + c].smr;
+            copy(Blk{B.sr.p + o, m.r, nrhs, B.sr.ld}, m);
+            o += m.r;
+          }
+          if (o != B.sr.r) throw Fail(AIFMM_ERR_NUMERIC, "children's multipole right-hand sides do not fill the parent's");
+          if ((int)ged.size() > 20000) flush_geam();
+        }
+        flush_geam();
+      }
+      forward_level(j);
+    }
+    solve_base_rhs(2);
+    for (int j = 2; j <= depth; ++j)
+      for (const auto& ks : bwd_waves[j]) backward_wave(j, ks);
     // gather the leaf particles
-    double2* dx = (flags & AIFMM_PTR_DEVICE) ? reinterpret_cast<double2*>(x) : static_cast<double2*>(pool.alloc(bytes));
+    double2* dx = dev ? reinterpret_cast<double2*>(x) : tx.as<double2>();
+    const long ldd_x = dev ? ldx : N;
     for (int k = 0; k < nBoxes[depth]; ++k) {
       const Blk& px = T[depth][k].particles;
-      Blk dst{dx + (size_t)k * rank, rank, nrhs, N};
+      Blk dst{dx + (size_t)k * rank, rank, nrhs, (int)ldd_x};
       if (px.r == rank) copy(dst, px);
       else zero(dst);
       if ((int)ged.size() > 20000) flush_geam();
     }
     flush_geam();
-    if (!(flags & AIFMM_PTR_DEVICE)) {
-      CK(cudaMemcpyAsync(x, dx, bytes, cudaMemcpyDeviceToHost, st));
-      sync();
-      pool.defer_free(dx, bytes);
-      pool.defer_free(db, bytes);
-    }
+    if (!dev)
+      CK(cudaMemcpy2DAsync(x, sizeof(double2) * ldx, dx, sizeof(double2) * N, sizeof(double2) * N, nrhs,
+                           cudaMemcpyDeviceToHost, st));
     sync();
+    release_solve_state();
     prof_collect();
     pool.commit_frees();
-    launches_fs = launches_ - l0;
+    launches_solve = launches_ - l0;
+    ms_solve = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+
+  void factorize_solve(int nrhs_, const double* b, double* x, int flags) {
+    if (nrhs_ < 1) throw Fail(AIFMM_ERR_ARG, "nrhs must be positive");
+    auto t0 = std::chrono::steady_clock::now();
+    factorize(flags);
+    solve_rhs(nrhs_, b, N, x, N, flags);
+    st_back_ms = ms_solve;
+    launches_fs = launches_factor + launches_solve;
     ms[3] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+
+  // ---- compressed matvec: y = A_c x with the kept pre-elimination assembly
+  //
+  // A_c is the matrix the assembly represents (the reference builds no such
+  // product; it is the operator whose blocks FMM2DTree_find_error.hpp:1105-1361
+  // and 1729-1741 assemble): the leaf near field P2P[k][nn] for the nine
+  // neighbours (self included) plus, at every level j, the interaction-list
+  // blocks L2P-chain M2L[k][kIL] P2M-chain.  With nested bases this is the H^2
+  // product: multipoles upward (leaf P2M x, then P2M of the concatenated
+  // children's multipoles), M2L at every level, locals downward (a parent's
+  // L2P times its locals adds to its children's locals, which are consecutive
+  // in Morton order), then L2P at the leaves plus the near field.
+  void compressed_matvec(const double2* x, long ldx, double2* y, long ldy, int nr) {
+    if (!have_saved) throw Fail(AIFMM_ERR_STATE, "the compressed product needs the kept assembly (AIFMM_KEEP_ASSEMBLY)");
+    std::vector<std::vector<int>> mo(depth + 1), lo(depth + 1);
+    std::vector<Blk> Mv(depth + 1), Lv(depth + 1);
+    for (int j = 2; j <= depth; ++j) {
+      int mt = 0, lt = 0;
+      mo[j].resize(nBoxes[j] + 1);
+      lo[j].resize(nBoxes[j] + 1);
+      for (int k = 0; k < nBoxes[j]; ++k) {
+        mo[j][k] = mt; mt += saved[j][k].NumM;
+        lo[j][k] = lt; lt += saved[j][k].NumL;
+      }
+      mo[j][nBoxes[j]] = mt;
+      lo[j][nBoxes[j]] = lt;
+      Mv[j] = scr(mt, nr);
+      Lv[j] = scr(lt, nr);
+    }
+    auto rows = [&](const Blk& v, int r0, int r1) { return Blk{v.p ? v.p + r0 : nullptr, r1 - r0, nr, v.ld}; };
+    // upward: multipoles
+    for (int k = 0; k < nBoxes[depth]; ++k) {
+      const Saved& S = saved[depth][k];
+      gemm(rows(Mv[depth], mo[depth][k], mo[depth][k + 1]), S.P2M, 0,
+           Blk{const_cast<double2*>(x) + (size_t)k * rank, rank, nr, (int)ldx}, 0, C1, C0);
+    }
+    flush_gemm();
+    for (int j = depth - 1; j >= 2; --j) {
+      for (int k = 0; k < nBoxes[j]; ++k)
+        gemm(rows(Mv[j], mo[j][k], mo[j][k + 1]), saved[j][k].P2M, 0,
+             rows(Mv[j + 1], mo[j + 1][4 * k], mo[j + 1][4 * k + 4]), 0, C1, C0);
+      flush_gemm();
+    }
+    // interaction lists: locals
+    for (int j = 2; j <= depth; ++j) {
+      for (int k = 0; k < nBoxes[j]; ++k) {
+        const Box& B = T[j][k];
+        std::vector<std::pair<Blk, Blk>> terms;
+        auto add = [&](int kIL) {
+          auto it = saved[j][k].M2L.find(kIL);
+          if (it == saved[j][k].M2L.end()) return;
+          terms.push_back({it->second, rows(Mv[j], mo[j][kIL], mo[j][kIL + 1])});
+        };
+        for (int i = 0; i < 16; ++i) if (B.inner[i] != -1) add(B.inner[i]);
+        for (int i = 0; i < 24; ++i) if (B.outer[i] != -1) add(B.outer[i]);
+        gemm_sum(rows(Lv[j], lo[j][k], lo[j][k + 1]), terms, C1, C0);
+        if ((int)gd.size() > 20000) flush_gemm();
+      }
+      flush_gemm();
+    }
+    // downward: a parent's L2P times its locals adds to its children's locals
+    for (int j = 2; j < depth; ++j) {
+      for (int k = 0; k < nBoxes[j]; ++k)
+        gemm(rows(Lv[j + 1], lo[j + 1][4 * k], lo[j + 1][4 * k + 4]), saved[j][k].L2P, 0,
+             rows(Lv[j], lo[j][k], lo[j][k + 1]), 0, C1, C1);
+      flush_gemm();
+    }
+    // leaves: near field plus L2P times the locals
+    for (int k = 0; k < nBoxes[depth]; ++k) {
+      const Box& B = T[depth][k];
+      const Saved& S = saved[depth][k];
+      std::vector<std::pair<Blk, Blk>> terms;
+      auto near = [&](int nn) {
+        auto it = S.P2P.find(nn);
+        if (it == S.P2P.end()) throw Fail(AIFMM_ERR_NUMERIC, "kept assembly lacks a leaf near-field block");
+        terms.push_back({it->second, Blk{const_cast<double2*>(x) + (size_t)nn * rank, rank, nr, (int)ldx}});
+      };
+      for (int n = 0; n < 8; ++n) if (B.nb[n] != -1) near(B.nb[n]);
+      near(k);
+      terms.push_back({S.L2P, rows(Lv[depth], lo[depth][k], lo[depth][k + 1])});
+      gemm_sum(Blk{y + (size_t)k * rank, rank, nr, (int)ldy}, terms, C1, C0);
+      if ((int)gd.size() > 20000) flush_gemm();
+    }
+    flush_gemm();
+    end_step();
+  }
+
+  // ---- GMRES refinement against the compressed product
+  //
+  // Right-preconditioned restarted GMRES on A_c x = b with the kept
+  // factorisation as the preconditioner M^-1 (solve_rhs), all in FP64: the
+  // factors may come from a looser recompression tolerance than the assembly
+  // (aifmm_set_factor_tolerance), the residual is always the assembly's.  The
+  // nrhs columns run as independent Krylov processes in lockstep; the
+  // Hessenberg matrices and Givens rotations live on the host.
+  int gm_iters = 0;
+  double gm_relres = 0;
+  void refine_solve(int nr, const double* b, long ldb, double* x, long ldx, int flags, double rtol, int maxit,
+                    int restart) {
+    if (!factored) throw Fail(AIFMM_ERR_STATE, "factorize() must run before a refined solve");
+    if (!have_saved) throw Fail(AIFMM_ERR_STATE, "a refined solve needs the kept assembly (factorize with AIFMM_KEEP_ASSEMBLY)");
+    if (nr < 1 || restart < 1 || maxit < 0 || !(rtol > 0)) throw Fail(AIFMM_ERR_ARG, "invalid refinement parameters");
+    if (ldb < N || ldx < N) throw Fail(AIFMM_ERR_ARG, "leading dimension smaller than the number of unknowns");
+    const bool dev = flags & AIFMM_PTR_DEVICE;
+    const size_t vb = sizeof(double2) * (size_t)N * nr;
+    const int m = restart;
+    Tmp tB(this, vb), tX(this, vb), tW(this, vb), tZ(this, vb), tV(this, vb * (m + 1));
+    Tmp tc(this, sizeof(double2) * nr * 2);
+    double2* B = tB.as<double2>();
+    double2* X = tX.as<double2>();
+    double2* W = tW.as<double2>();
+    double2* Z = tZ.as<double2>();
+    double2* V = tV.as<double2>();
+    double2* dcoef = tc.as<double2>();
+    auto Vi = [&](int i) { return V + (size_t)i * N * nr; };
+    if (dev) CK(cudaMemcpy2DAsync(B, sizeof(double2) * N, b, sizeof(double2) * ldb, sizeof(double2) * N, nr,
+                                  cudaMemcpyDeviceToDevice, st));
+    else CK(cudaMemcpy2DAsync(B, sizeof(double2) * N, b, sizeof(double2) * ldb, sizeof(double2) * N, nr,
+                              cudaMemcpyHostToDevice, st));
+    auto dots = [&](const double2* a, const double2* c, std::vector<double2>& out) {
+      int e = aifmm_launch_coldot(a, N, c, N, N, nr, dcoef, st);
+      if (e) throw Fail(AIFMM_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
+      out.resize(nr);
+      d2h(out.data(), dcoef, sizeof(double2) * nr);
+    };
+    // y(:,c) = alpha_c x(:,c) + beta_c y(:,c)
+    auto axpby = [&](const double2* xx, double2* yy, const std::vector<double2>& al, const std::vector<double2>& be) {
+      std::vector<double2> ab(2 * nr);
+      for (int c = 0; c < nr; ++c) { ab[c] = al[c]; ab[nr + c] = be[c]; }
+      const double2* dab = static_cast<const double2*>(stage.put_raw(ab.data(), sizeof(double2) * 2 * nr, st));
+      int e = aifmm_launch_colaxpby(xx, N, yy, N, N, nr, dab, dab + nr, st);
+      if (e) throw Fail(AIFMM_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
+    };
+    auto precond = [&](const double2* in, double2* out) {  // out = M^-1 in
+      solve_rhs(nr, reinterpret_cast<const double*>(in), N, reinterpret_cast<double*>(out), N, AIFMM_PTR_DEVICE);
+    };
+    const std::vector<double2> one(nr, C1), mone(nr, CM1), zero_(nr, C0);
+    std::vector<double2> d;
+    dots(B, B, d);
+    std::vector<double> bn(nr);
+    for (int c = 0; c < nr; ++c) bn[c] = std::sqrt(d[c].x) > 0 ? std::sqrt(d[c].x) : 1.0;
+    precond(B, X);  // the direct solve is the starting guess
+    int it = 0;
+    double worst = 0;
+    for (;;) {
+      // true residual r = b - A_c x into V_0
+      compressed_matvec(X, N, W, N, nr);
+      CK(cudaMemcpyAsync(Vi(0), B, vb, cudaMemcpyDeviceToDevice, st));
+      axpby(W, Vi(0), mone, one);
+      dots(Vi(0), Vi(0), d);
+      std::vector<double> beta(nr);
+      worst = 0;
+      for (int c = 0; c < nr; ++c) { beta[c] = std::sqrt(d[c].x); worst = std::max(worst, beta[c] / bn[c]); }
+      if (worst <= rtol || it >= maxit) break;
+      {
+        std::vector<double2> sc(nr);
+        for (int c = 0; c < nr; ++c) sc[c] = make_double2(beta[c] > 0 ? 1.0 / beta[c] : 0.0, 0.0);
+        axpby(Vi(0), Vi(0), zero_, sc);
+      }
+      // per column: H (m+1) x m column-major, Givens (cs, sn), g
+      std::vector<std::vector<double2>> H(nr, std::vector<double2>((size_t)(m + 1) * m, C0));
+      std::vector<std::vector<double>> cs(nr, std::vector<double>(m));
+      std::vector<std::vector<double2>> sn(nr, std::vector<double2>(m)), g(nr, std::vector<double2>(m + 1, C0));
+      for (int c = 0; c < nr; ++c) g[c][0] = make_double2(beta[c], 0.0);
+      int k = 0;
+      for (; k < m && it < maxit; ++k, ++it) {
+        precond(Vi(k), Z);
+        compressed_matvec(Z, N, W, N, nr);
+        for (int l = 0; l <= k; ++l) {  // modified Gram-Schmidt
+          dots(Vi(l), W, d);
+          std::vector<double2> neg(nr);
+          for (int c = 0; c < nr; ++c) { H[c][l + (size_t)k * (m + 1)] = d[c]; neg[c] = make_double2(-d[c].x, -d[c].y); }
+          axpby(Vi(l), W, neg, one);
+        }
+        dots(W, W, d);
+        std::vector<double2> sc(nr);
+        double est = 0;
+        for (int c = 0; c < nr; ++c) {
+          const double h1 = std::sqrt(d[c].x);
+          H[c][k + 1 + (size_t)k * (m + 1)] = make_double2(h1, 0.0);
+          sc[c] = make_double2(h1 > 1e-300 ? 1.0 / h1 : 0.0, 0.0);
+          // apply the previous rotations to column k, then a new one that zeroes H(k+1, k)
+          double2* hk = &H[c][(size_t)k * (m + 1)];
+          for (int l = 0; l < k; ++l) {
+            const double2 a = hk[l], bb = hk[l + 1];
+            const double2 s_ = sn[c][l];
+            // [c s; -conj(s) c] [a; b]
+            hk[l] = make_double2(cs[c][l] * a.x + (s_.x * bb.x - s_.y * bb.y), cs[c][l] * a.y + (s_.x * bb.y + s_.y * bb.x));
+            hk[l + 1] = make_double2(cs[c][l] * bb.x - (s_.x * a.x + s_.y * a.y), cs[c][l] * bb.y - (s_.x * a.y - s_.y * a.x));
+          }
+          const double2 a = hk[k], bb = hk[k + 1];
+          const double na = std::hypot(a.x, a.y), nb = std::hypot(bb.x, bb.y);
+          if (nb == 0.0) { cs[c][k] = 1.0; sn[c][k] = C0; }
+          else if (na == 0.0) { cs[c][k] = 0.0; sn[c][k] = make_double2(bb.x / nb, -bb.y / nb); }
+          else {
+            const double r = std::hypot(na, nb);
+            cs[c][k] = na / r;
+            // s = (a / |a|) conj(b) / r
+            const double2 u = make_double2(a.x / na, a.y / na);
+            sn[c][k] = make_double2((u.x * bb.x + u.y * bb.y) / r, (u.y * bb.x - u.x * bb.y) / r);
+          }
+          const double2 a2 = hk[k];
+          const double2 s_ = sn[c][k];
+          hk[k] = make_double2(cs[c][k] * a2.x + (s_.x * bb.x - s_.y * bb.y), cs[c][k] * a2.y + (s_.x * bb.y + s_.y * bb.x));
+          hk[k + 1] = C0;
+          const double2 gk = g[c][k];
+          g[c][k] = make_double2(cs[c][k] * gk.x, cs[c][k] * gk.y);
+          g[c][k + 1] = make_double2(-(s_.x * gk.x + s_.y * gk.y), -(s_.x * gk.y - s_.y * gk.x));
+          est = std::max(est, std::hypot(g[c][k + 1].x, g[c][k + 1].y) / bn[c]);
+        }
+        axpby(W, Vi(k + 1), sc, zero_);
+        if (est <= rtol) { ++k; ++it; break; }
+      }
+      // y = R^-1 g (back substitution per column), u = V y, x += M^-1 u
+      CK(cudaMemsetAsync(W, 0, vb, st));
+      std::vector<std::vector<double2>> yv(nr, std::vector<double2>(k, C0));
+      for (int c = 0; c < nr; ++c)
+        for (int l = k - 1; l >= 0; --l) {
+          double2 sum = g[c][l];
+          for (int q = l + 1; q < k; ++q) sum = csub(sum, cmul(H[c][l + (size_t)q * (m + 1)], yv[c][q]));
+          const double2 dd = H[c][l + (size_t)l * (m + 1)];
+          yv[c][l] = (dd.x == 0.0 && dd.y == 0.0) ? C0 : cdiv(sum, dd);
+        }
+      for (int l = 0; l < k; ++l) {
+        std::vector<double2> al(nr);
+        for (int c = 0; c < nr; ++c) al[c] = yv[c][l];
+        axpby(Vi(l), W, al, one);
+      }
+      precond(W, Z);
+      axpby(Z, X, one, one);
+    }
+    gm_iters = it;
+    gm_relres = worst;
+    if (dev) CK(cudaMemcpy2DAsync(x, sizeof(double2) * ldx, X, sizeof(double2) * N, sizeof(double2) * N, nr,
+                                  cudaMemcpyDeviceToDevice, st));
+    else CK(cudaMemcpy2DAsync(x, sizeof(double2) * ldx, X, sizeof(double2) * N, sizeof(double2) * N, nr,
+                              cudaMemcpyDeviceToHost, st));
+    sync();
+    pool.commit_frees();
   }
 
   // Saved copy of the assembled state (L2P, P2M, M2L, leaf P2P) so that
@@ -2344,8 +2775,9 @@ aifmm_status aifmm_tables_compute(aifmm_problem* p, int round6_) {
 aifmm_status aifmm_tables_set(aifmm_problem* p, const double* M, const double* near_tables) {
   if (!p || !M || !near_tables) return AIFMM_ERR_ARG;
   return guard(p, [&] {
-    CK(cudaMemcpy(p->d_M, M, sizeof(double2) * 121 * p->rank, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(p->d_near, near_tables, sizeof(double2) * 9 * p->rank * p->rank, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(p->d_M, M, sizeof(double2) * 121 * p->rank, cudaMemcpyHostToDevice, p->st));
+    CK(cudaMemcpyAsync(p->d_near, near_tables, sizeof(double2) * 9 * p->rank * p->rank, cudaMemcpyHostToDevice, p->st));
+    p->sync();
     p->tables_ready = true;
   });
 }
@@ -2355,8 +2787,8 @@ aifmm_status aifmm_tables_get(aifmm_problem* p, double* M, double* near_tables) 
   if (!p->tables_ready) { p->err = "tables not ready"; return AIFMM_ERR_STATE; }
   return guard(p, [&] {
     p->sync();
-    CK(cudaMemcpy(M, p->d_M, sizeof(double2) * 121 * p->rank, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(near_tables, p->d_near, sizeof(double2) * 9 * p->rank * p->rank, cudaMemcpyDeviceToHost));
+    p->d2h(M, p->d_M, sizeof(double2) * 121 * p->rank);
+    p->d2h(near_tables, p->d_near, sizeof(double2) * 9 * p->rank * p->rank);
   });
 }
 
@@ -2370,7 +2802,7 @@ aifmm_status aifmm_grid_points(aifmm_problem* p, double* xy) {
   if (!p || !xy) return AIFMM_ERR_ARG;
   return guard(p, [&] {
     p->sync();
-    CK(cudaMemcpy(xy, p->d_pts, sizeof(double2) * p->N, cudaMemcpyDeviceToHost));
+    p->d2h(xy, p->d_pts, sizeof(double2) * p->N);
   });
 }
 
@@ -2453,6 +2885,156 @@ aifmm_status aifmm_factorize_solve(aifmm_problem* p, int nrhs, const double* b, 
   return guard(p, [&] { p->factorize_solve(nrhs, b, x, flags); });
 }
 
+aifmm_status aifmm_factorize(aifmm_problem* p, int precision, int flags) {
+  if (!p) return AIFMM_ERR_ARG;
+  if (precision != AIFMM_PRECISION_FP64) {
+    p->err = "only AIFMM_PRECISION_FP64 factorisations are available";
+    return AIFMM_ERR_ARG;
+  }
+  return guard(p, [&] { p->factorize(flags); });
+}
+
+aifmm_status aifmm_solve(aifmm_problem* p, int nrhs, const double* b, long ldb, double* x, long ldx, void* stream,
+                         int flags) {
+  if (!p || !b || !x || nrhs < 1) return AIFMM_ERR_ARG;
+  return guard(p, [&] {
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    if (cs) {  // the solve starts after the work already queued on the caller's stream
+      CK(cudaEventRecord(p->ev_fork, cs));
+      CK(cudaStreamWaitEvent(p->st, p->ev_fork, 0));
+    }
+    p->solve_rhs(nrhs, b, ldb, x, ldx, flags);
+    p->st_back_ms = p->ms_solve;
+    if (cs) {  // and the caller's stream sees the solution
+      CK(cudaEventRecord(p->ev_join, p->st));
+      CK(cudaStreamWaitEvent(cs, p->ev_join, 0));
+    }
+  });
+}
+
+aifmm_status aifmm_set_factor_tolerance(aifmm_problem* p, int tol_pow) {
+  if (!p || tol_pow < 0 || tol_pow > 15) return AIFMM_ERR_ARG;
+  p->tol_factor = tol_pow == 0 ? p->tol : std::pow(10, -1.0 * tol_pow);
+  return AIFMM_OK;
+}
+
+aifmm_status aifmm_compressed_matvec(aifmm_problem* p, int nrhs, const double* x, long ldx, double* y, long ldy,
+                                     int flags) {
+  if (!p || !x || !y || nrhs < 1) return AIFMM_ERR_ARG;
+  if (ldx < p->N || ldy < p->N) return AIFMM_ERR_ARG;
+  return guard(p, [&] {
+    const bool dev = flags & AIFMM_PTR_DEVICE;
+    const long N = p->N;
+    const size_t bytes = sizeof(double2) * (size_t)N * nrhs;
+    aifmm_problem::Tmp tx(p, dev ? 1 : bytes), ty(p, dev ? 1 : bytes);
+    const double2* dx = reinterpret_cast<const double2*>(x);
+    double2* dy = reinterpret_cast<double2*>(y);
+    long lx = ldx, ly = ldy;
+    if (!dev) {
+      CK(cudaMemcpy2DAsync(tx.ptr, sizeof(double2) * N, x, sizeof(double2) * ldx, sizeof(double2) * N, nrhs,
+                           cudaMemcpyHostToDevice, p->st));
+      dx = tx.as<double2>(); dy = ty.as<double2>();
+      lx = ly = N;
+    }
+    p->cur = p->st;
+    p->nrhs = nrhs;
+    p->compressed_matvec(dx, lx, dy, ly, nrhs);
+    if (!dev)
+      CK(cudaMemcpy2DAsync(y, sizeof(double2) * ldy, dy, sizeof(double2) * N, sizeof(double2) * N, nrhs,
+                           cudaMemcpyDeviceToHost, p->st));
+    p->sync();
+  });
+}
+
+aifmm_status aifmm_solve_refined(aifmm_problem* p, int nrhs, const double* b, long ldb, double* x, long ldx,
+                                 double rtol, int maxit, int* iterations, double* relres, int flags) {
+  if (!p || !b || !x || nrhs < 1) return AIFMM_ERR_ARG;
+  return guard(p, [&] {
+    p->cur = p->st;
+    p->refine_solve(nrhs, b, ldb, x, ldx, flags, rtol, maxit, 30);
+    if (iterations) *iterations = p->gm_iters;
+    if (relres) *relres = p->gm_relres;
+  });
+}
+
+aifmm_status aifmm_find_error(aifmm_problem* p, int nrhs, const double* x, long ldx, const double* x_true, long ldt,
+                              double* rel, int flags) {
+  if (!p || !x || !x_true || !rel || nrhs < 1) return AIFMM_ERR_ARG;
+  if (ldx < p->N || ldt < p->N) return AIFMM_ERR_ARG;
+  return guard(p, [&] {
+    const long N = p->N;
+    double se = 0.0, st = 0.0;
+    if (flags & AIFMM_PTR_DEVICE) {
+      aifmm_problem::Tmp part(p, aifmm_error_norms_scratch_bytes()), out(p, 2 * sizeof(double));
+      int e = aifmm_launch_error_norms(reinterpret_cast<const double2*>(x), ldx,
+                                       reinterpret_cast<const double2*>(x_true), ldt, N, nrhs, part.as<double>(),
+                                       out.as<double>(), p->st);
+      if (e) throw Fail(AIFMM_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
+      double h[2];
+      CK(cudaMemcpyAsync(h, out.ptr, sizeof h, cudaMemcpyDeviceToHost, p->st));
+      p->sync();
+      se = h[0];
+      st = h[1];
+    } else {
+      for (int c = 0; c < nrhs; ++c)
+        for (long i = 0; i < N; ++i) {
+          const double* a = x + 2 * (i + c * ldx);
+          const double* t = x_true + 2 * (i + c * ldt);
+          se += (a[0] - t[0]) * (a[0] - t[0]) + (a[1] - t[1]) * (a[1] - t[1]);
+          st += t[0] * t[0] + t[1] * t[1];
+        }
+    }
+    *rel = std::sqrt(se) / std::sqrt(st);
+  });
+}
+
+aifmm_status aifmm_trim(aifmm_problem* p) {
+  if (!p) return AIFMM_ERR_ARG;
+  return guard(p, [&] {
+    p->sync();
+    CK(cudaStreamSynchronize(p->st2));
+    p->gb_idx.release(); p->gb_lst.release(); p->gb_segs.release();
+    p->gb_ws.release(); p->gb_res.release(); p->gb_lu.release();
+    if (p->have_saved) p->release_saved();
+    p->have_saved = false;
+    p->pool.commit_frees();
+  });
+}
+
+aifmm_status aifmm_zgemm(aifmm_problem* p, int opA, int opB, int m, int n, int k, const double* alpha,
+                         const double* A, int lda, const double* B, int ldb, const double* beta, double* C, int ldc,
+                         int flags) {
+  if (!p || !alpha || !beta || m < 0 || n < 0 || k < 0 || (opA != 0 && opA != 1) || (opB != 0 && opB != 1))
+    return AIFMM_ERR_ARG;
+  const int ar = opA ? k : m, ac = opA ? m : k, br = opB ? n : k, bc = opB ? k : n;
+  if (lda < std::max(1, ar) || ldb < std::max(1, br) || ldc < std::max(1, m)) return AIFMM_ERR_ARG;
+  if ((long)m * n > 0 && (!C || ((long)k > 0 && (!A || !B)))) return AIFMM_ERR_ARG;
+  return guard(p, [&] {
+    if ((long)m * n == 0) return;
+    const bool dev = flags & AIFMM_PTR_DEVICE;
+    const size_t bA = sizeof(double2) * (size_t)lda * ac, bB = sizeof(double2) * (size_t)ldb * bc;
+    const size_t bC = sizeof(double2) * (size_t)ldc * n;
+    aifmm_problem::Tmp tA(p, dev ? 1 : bA), tB(p, dev ? 1 : bB), tC(p, dev ? 1 : bC);
+    double2* dA = reinterpret_cast<double2*>(const_cast<double*>(A));
+    double2* dB = reinterpret_cast<double2*>(const_cast<double*>(B));
+    double2* dC = reinterpret_cast<double2*>(C);
+    if (!dev) {
+      if (k > 0) {
+        CK(cudaMemcpyAsync(tA.ptr, A, bA, cudaMemcpyHostToDevice, p->st));
+        CK(cudaMemcpyAsync(tB.ptr, B, bB, cudaMemcpyHostToDevice, p->st));
+      }
+      CK(cudaMemcpyAsync(tC.ptr, C, bC, cudaMemcpyHostToDevice, p->st));
+      dA = tA.as<double2>(); dB = tB.as<double2>(); dC = tC.as<double2>();
+    }
+    Blk a{dA, ar, ac, lda}, b{dB, br, bc, ldb}, c{dC, m, n, ldc};
+    p->cur = p->st;
+    p->gemm(c, a, opA, b, opB, make_double2(alpha[0], alpha[1]), make_double2(beta[0], beta[1]));
+    p->flush_gemm();
+    if (!dev) CK(cudaMemcpyAsync(C, dC, bC, cudaMemcpyDeviceToHost, p->st));
+    p->sync();
+  });
+}
+
 aifmm_status aifmm_dense_matvec(aifmm_problem* p, int nrhs, const double* x, double* y, int flags) {
   if (!p || !x || !y || nrhs < 1 || nrhs > 8) return AIFMM_ERR_ARG;
   if (!p->tables_ready) { p->err = "tables not ready"; return AIFMM_ERR_STATE; }
@@ -2516,6 +3098,8 @@ aifmm_status aifmm_box_skeleton(aifmm_problem* p, int level, int box, int which,
 aifmm_status aifmm_phase_times(const aifmm_problem* p, double* ms) {
   if (!p || !ms) return AIFMM_ERR_ARG;
   for (int i = 0; i < 4; ++i) ms[i] = p->ms[i];
+  ms[4] = p->ms_factor;
+  ms[5] = p->ms_solve;
   return AIFMM_OK;
 }
 
@@ -2523,6 +3107,13 @@ aifmm_status aifmm_launch_counts(const aifmm_problem* p, long* factor_solve, lon
   if (!p || !factor_solve || !assemble) return AIFMM_ERR_ARG;
   *factor_solve = p->launches_fs;
   *assemble = p->launches_asm;
+  return AIFMM_OK;
+}
+
+aifmm_status aifmm_launch_counts_split(const aifmm_problem* p, long* factorize, long* solve) {
+  if (!p || !factorize || !solve) return AIFMM_ERR_ARG;
+  *factorize = p->launches_factor;
+  *solve = p->launches_solve;
   return AIFMM_OK;
 }
 
@@ -2548,7 +3139,8 @@ aifmm_status aifmm_kernel_profile_read(aifmm_problem* p, int kind, long* launche
 aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n) {
   if (!p || !out) return AIFMM_ERR_ARG;
   const double grow = (double)(p->gb_idx.capacity() + p->gb_lst.capacity() + p->gb_segs.capacity() +
-                               p->gb_ws.capacity() + p->gb_res.capacity() + p->gb_lu.capacity());
+                               p->gb_ws.capacity() + p->gb_res.capacity() + p->gb_lu.capacity() +
+                               p->scratch.capacity() + p->stage.cap_);
   const double v[15] = {p->st_sync_ms, (double)p->st_syncs, p->st_pending_ms, p->st_elim_ms, p->st_back_ms,
                         (double)p->st_compress, p->ms[3], (double)p->launches_fs,
                         p->st_asm_lists_ms, p->st_asm_aca_ms, p->st_asm_lu_ms, p->st_asm_blocks_ms,

@@ -239,6 +239,9 @@ def main():
     ap.add_argument("--depth", type=int, default=WORKLOAD["depth"], help="override the tree depth (diagnostics)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")
+    ap.add_argument("--no-serving", action="store_true", help="skip the solve-latency measurement with kept factors")
+    ap.add_argument("--batched", type=int, default=1, help="1: also run the 64-problem batched configuration")
+    ap.add_argument("--trace", type=float, default=60.0, help="seconds of the serving trace (0: skip)")
     ap.add_argument("--no-kernel-profile", action="store_true",
                     help="skip the extra event-instrumented step that feeds the roofline (profiling runs)")
     args = ap.parse_args()
@@ -344,6 +347,18 @@ def main():
             t_e2e = float(tt.item())
     x = (x_pin if t_e2e is not None else x_dev.cpu()).numpy().view(np.complex128).reshape(NRHS, N)
     finite = bool(np.isfinite(x).all())
+    serving = None if args.no_serving else solve_latency(T, K, lib, stream, device, args)
+    extra = {}
+    if args.batched and rank == 0:
+        try:
+            extra["batched_uneven"] = batched_uneven(device)
+        except Exception as e:  # reported, never fatal for the headline measurement
+            extra["batched_uneven"] = {"error": repr(e)}
+    if args.trace > 0 and rank == 0:
+        try:
+            extra["serving_trace"] = serving_trace(device, seconds=args.trace)
+        except Exception as e:
+            extra["serving_trace"] = {"error": repr(e)}
     # one more step, untimed, with CUDA events around every launch of the dense
     # kernels: per-kernel durations and algorithmic flops for the roofline
     kinds = {0: "qr_factor", 1: "qr_solve", 2: "gemm"}
@@ -375,6 +390,8 @@ def main():
             "solver_stats_last_step": solver_stats,
             "clocks": clk,
             "solution_finite": finite,
+            "solves_with_cached_factors": serving,
+            **extra,
         }
         if not args.no_cpu_baseline and ws == 1:
             line["cpu_baseline"] = cpu_baseline_sample()
@@ -383,6 +400,159 @@ def main():
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def solve_latency(T, K, lib, stream, device, args, nrhs_list=(1, 8, 64)):
+    """Latency of aifmm_solve against factors kept on the device (one factorisation,
+    then W untimed and K timed solves per right-hand-side count; right-hand sides
+    and solutions resident in HBM).  Each solve is bracketed by CUDA events on the
+    solver's stream."""
+    import ctypes
+    import torch
+    T.createTree()
+    T.assemble()
+    t0 = time.perf_counter()
+    T.factorize()
+    t_factor = time.perf_counter() - t0
+    N = K.N
+    out = {"factorize_ms": 1e3 * t_factor, "unknowns": N}
+    rng = np.random.default_rng(SEED + 7)
+    dp = ctypes.POINTER(ctypes.c_double)
+    for nr in nrhs_list:
+        th = rng.uniform(0, 2 * np.pi, nr)
+        b = torch.from_numpy(K.rhs_plane_wave(th).view(np.float64).copy()).to(f"cuda:{device}")
+        x = torch.empty_like(b)
+        ms = []
+        launches = 0
+        for it in range(args.warmup + args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = lib.aifmm_solve(K.h, nr, ctypes.cast(b.data_ptr(), dp), N, ctypes.cast(x.data_ptr(), dp), N, None, 1)
+            e1.record(stream)
+            if st != 0:
+                raise RuntimeError(lib.aifmm_last_error(K.h).decode())
+            e1.synchronize()
+            if it >= args.warmup:
+                ms.append(e0.elapsed_time(e1))
+                launches = T.launch_counts_split()[1]
+        ms = np.array(ms)
+        out["nrhs_%d" % nr] = {"p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
+                               "mean_ms": float(ms.mean()), "solves": int(ms.size),
+                               "rhs_unknowns_per_s": float(N * nr / (ms.mean() * 1e-3)),
+                               "gpu_launches_per_solve": int(launches)}
+        del b, x
+    return out
+
+
+def _random_problem(rng, depth):
+    """A problem of the batched / serving configurations: 6x6 nodes, kappa log-uniform in
+    [5, 60], contrast a Gaussian of amplitude U[0.5, 2] (width 32) or a disk of radius
+    U[0.2, 0.7] (amplitude 2), NCA tolerance 1e-8."""
+    kappa = float(np.exp(rng.uniform(np.log(5.0), np.log(60.0))))
+    if rng.uniform() < 0.5:
+        q = dict(q_kind="gauss_aw", q_amp=float(rng.uniform(0.5, 2.0)), q_width=32.0)
+    else:
+        q = dict(q_kind="disk", q_amp=2.0, q_radius=float(rng.uniform(0.2, 0.7)))
+    return dict(n_cheb=6, kappa=kappa, degree=6, depth=int(depth), tol_pow=8, **q)
+
+
+def batched_uneven(device, nprob=64, workers=4, seed=SEED + 3):
+    """64 independent problems of depth U{4..7}, each factored and solved for one random
+    complex Gaussian right-hand side, run through the serving engine (workers drive their
+    own handles and streams, so the problems overlap on the GPU; admission by device
+    memory).  Whole-job unknowns/s = total unknowns / wall time of the batch."""
+    import aifmm_ls_b200 as A
+    rng = np.random.default_rng(seed)
+    probs = [_random_problem(rng, rng.integers(4, 8)) for _ in range(nprob)]
+    S = A.Server(device=device, workers=workers, max_batch_rhs=64)
+    try:
+        t0 = time.perf_counter()
+        fids = [S.factorize(i, **kw) for i, kw in enumerate(probs)]
+        sids = []
+        for i, kw in enumerate(probs):
+            N = 4 ** kw["depth"] * 36
+            b = rng.standard_normal((1, N)) + 1j * rng.standard_normal((1, N))
+            sids.append(S.solve(i, b))
+        bad = 0
+        for r in fids + sids:
+            st = S.wait(r, timeout=3600)[0]
+            bad += st != 0
+        wall = time.perf_counter() - t0
+        stats = S.stats()
+    finally:
+        S.close()
+    unknowns = sum(4 ** kw["depth"] * 36 for kw in probs)
+    depths = [kw["depth"] for kw in probs]
+    return {"problems": nprob, "depth_counts": {str(d): depths.count(d) for d in range(4, 8)},
+            "unknowns": unknowns, "wall_s": wall, "unknowns_per_s": unknowns / wall, "failed": bad,
+            "workers": workers, "timing": "host wall clock around the whole batch (several streams)",
+            "server": stats}
+
+
+def serving_trace(device, seconds=60.0, rate=200.0, workers=4, seed=SEED + 4):
+    """Poisson arrivals at `rate` req/s for `seconds`: 5% factorize requests for new
+    geometries (depth U{5,6}, problem as the batched configuration), 95% solve requests
+    of U{1..64} plane waves against a random resident geometry.  Latency = submission to
+    completion (host clock); the engine batches the solves queued for a geometry."""
+    import aifmm_ls_b200 as A
+    rng = np.random.default_rng(seed)
+    S = A.Server(device=device, workers=workers, max_batch_rhs=64)
+    lat = {"solve": [], "factorize": []}
+    try:
+        keys = []
+        # a few geometries resident before the clock starts
+        for key in range(4):
+            kw = _random_problem(rng, rng.integers(5, 7))
+            S.wait(S.factorize(key, **kw), timeout=3600)
+            keys.append((key, kw))
+        Ks = {}
+        pending = []
+        t0 = time.perf_counter()
+        t_next = t0
+        nreq = 0
+        solved_unknowns = 0
+        while True:
+            now = time.perf_counter()
+            if now - t0 >= seconds:
+                break
+            if now < t_next:
+                time.sleep(min(t_next - now, 0.002))
+                continue
+            t_next += rng.exponential(1.0 / rate)
+            nreq += 1
+            if rng.uniform() < 0.05:
+                key = len(keys)
+                kw = _random_problem(rng, rng.integers(5, 7))
+                keys.append((key, kw))
+                pending.append(("factorize", S.factorize(key, **kw), 0))
+            else:
+                key, kw = keys[int(rng.integers(0, min(len(keys), 4 + len(keys) // 2)))]
+                if key not in Ks:
+                    Ks[key] = A.LSKernel(**kw)
+                nr = int(rng.integers(1, 65))
+                b = Ks[key].rhs_plane_wave(rng.uniform(0, 2 * np.pi, nr))
+                pending.append(("solve", S.solve(key, b), b.size))
+        failed = 0
+        for kind, rid, nunk in pending:
+            st, ms, br, _ = S.wait(rid, timeout=3600)
+            if st == 0:
+                lat[kind].append(ms)
+                solved_unknowns += nunk
+            else:
+                failed += 1
+        wall = time.perf_counter() - t0
+        stats = S.stats()
+    finally:
+        S.close()
+    out = {"seconds": seconds, "rate_req_per_s": rate, "requests": nreq, "failed": failed, "wall_s": wall,
+           "rhs_unknowns_per_s": solved_unknowns / wall, "server": stats,
+           "note": "trace shortened from 10 minutes; factorize depths 5-6 (a depth-7 factorisation takes "
+                   "seconds, far longer than the mean gap between factorize requests at 5% of 200 req/s)"}
+    for kind, v in lat.items():
+        if v:
+            out[kind] = {"count": len(v), "p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99))}
+    return out
 
 
 def roofline(prof, fp64_peak, t_dev):

@@ -34,9 +34,13 @@ typedef enum {
 } aifmm_status;
 
 enum { AIFMM_PTR_HOST = 0, AIFMM_PTR_DEVICE = 1,
-       /* factorize_solve: keep a copy of the assembled blocks so that the handle can be
-        * solved again without re-assembling (the elimination consumes them otherwise) */
+       /* factorize / factorize_solve: keep a copy of the assembled blocks so that the
+        * handle can be factored again without re-assembling (the elimination consumes
+        * them otherwise) */
        AIFMM_KEEP_ASSEMBLY = 2 };
+
+/* Factorisation precision (aifmm_factorize). */
+enum { AIFMM_PRECISION_FP64 = 0 };
 
 /* Contrast functions q(x): 0..5 are the reference's Qchoice values
  * (LS/LS_functions.hpp:99-112: gaussian 1.5 exp(-160|x|^2), multipleGaussians,
@@ -121,6 +125,65 @@ aifmm_status aifmm_assemble(aifmm_problem* p);
  * b and x are N x nrhs complex (column-major). */
 aifmm_status aifmm_factorize_solve(aifmm_problem* p, int nrhs, const double* b, double* x, int flags);
 
+/* FMM2DTree::eliminate_phase_efficient and the base-level factorisation of
+ * solve_particles_at_base_level (FMM2DTree_find_error.hpp:2407-2485) without a
+ * right-hand side: the factors (QR of every P2P[k][k] and L2M_f, the fill-in
+ * blocks the right-hand side passes through, the base-level QR) stay on the
+ * device until the next build_tree / assemble / factorize.  precision:
+ * AIFMM_PRECISION_FP64.  flags: AIFMM_KEEP_ASSEMBLY. */
+aifmm_status aifmm_factorize(aifmm_problem* p, int precision, int flags);
+/* The right-hand-side half of the reference's solve with kept factors:
+ * assign_Leaf_rhs, the right-hand-side updates of eliminate_x / eliminate_z
+ * (FMM2DTree_find_error.hpp:1968, 1997-2001, 2252, 2289-2293), the base-level
+ * solve (:2453-2485) and back_substitution_phase (:2487-2532), for nrhs
+ * right-hand sides at once.  b and x are N x nrhs complex with column strides ldb
+ * and ldx (>= N), host or device memory (flags).  Any number of solves may follow
+ * one aifmm_factorize.  stream (a cudaStream_t, may be NULL): the solve starts after
+ * the work already queued on it, and work queued on it afterwards sees x. */
+aifmm_status aifmm_solve(aifmm_problem* p, int nrhs, const double* b, long ldb, double* x, long ldx, void* stream,
+                         int flags);
+/* No counterpart in the reference: the recompression tolerance of the next
+ * factorisations, 10^-tol_pow (0: the description's tol_pow, which always stays the
+ * assembly's ACA tolerance).  A looser factorisation is a cheaper preconditioner for
+ * aifmm_solve_refined. */
+aifmm_status aifmm_set_factor_tolerance(aifmm_problem* p, int tol_pow);
+/* No counterpart in the reference (its hybrid.cpp:199 calls a matvec of a DFMM class
+ * that is not in the repository): y = A_c x, the product with the compressed matrix
+ * the assembly represents -- leaf near-field blocks plus the interaction-list M2L
+ * blocks of every level through the nested L2P / P2M bases (FMM2DTree_find_error.hpp:
+ * 1105-1361, 1729-1741) -- in FP64.  Needs the kept assembly: call after
+ * aifmm_factorize(p, precision, AIFMM_KEEP_ASSEMBLY).  x, y: N x nrhs complex with
+ * column strides ldx, ldy; host or device memory (flags). */
+aifmm_status aifmm_compressed_matvec(aifmm_problem* p, int nrhs, const double* x, long ldx, double* y, long ldy,
+                                     int flags);
+/* No counterpart in the reference: right-preconditioned restarted GMRES (restart 30) on
+ * A_c x = b in FP64, with the kept factorisation as the preconditioner and the direct
+ * solve as the starting guess, until every column's relative residual
+ * ||b - A_c x|| / ||b|| <= rtol or maxit preconditioned products.  Needs
+ * aifmm_factorize(p, precision, AIFMM_KEEP_ASSEMBLY).  *iterations and *relres (the
+ * worst column's final relative residual) may be NULL.  b, x as aifmm_solve. */
+aifmm_status aifmm_solve_refined(aifmm_problem* p, int nrhs, const double* b, long ldb, double* x, long ldx,
+                                 double rtol, int maxit, int* iterations, double* relres, int flags);
+/* FMM2DTree::error_check (FMM2DTree_find_error.hpp:2534-2581): *rel = ||x - x_true|| /
+ * ||x_true|| (Frobenius norms over the nrhs columns; x and x_true N x nrhs complex with
+ * column strides ldx and ldt, host or device memory). */
+aifmm_status aifmm_find_error(aifmm_problem* p, int nrhs, const double* x, long ldx, const double* x_true, long ldt,
+                              double* rel, int flags);
+
+/* No counterpart in the reference: return the assembly's reusable workspaces and the
+ * kept copy of the assembled blocks (AIFMM_KEEP_ASSEMBLY) to the device, keeping the
+ * factors.  For a handle that from now on only solves (a cached factorisation). */
+aifmm_status aifmm_trim(aifmm_problem* p);
+
+/* No counterpart in the reference (its products are Eigen expressions inside the
+ * elimination, e.g. FMM2DTree_find_error.hpp:1961-2075): the solver's batched complex
+ * GEMM kernel (FP64 tensor cores) on one product, C = alpha op(A) op(B) + beta C,
+ * op 0 = as is, 1 = conjugate transpose; column-major, alpha and beta are one
+ * complex number each (host).  For checking the kernel against another BLAS. */
+aifmm_status aifmm_zgemm(aifmm_problem* p, int opA, int opB, int m, int n, int k, const double* alpha,
+                         const double* A, int lda, const double* B, int ldb, const double* beta, double* C, int ldc,
+                         int flags);
+
 /* The dense product of the find_error fixture generator (FMM2DTree_gen_rhs_x.hpp:2864-2871):
  * y = A x with exact entries, x and y N x nrhs complex (nrhs <= 8). */
 aifmm_status aifmm_dense_matvec(aifmm_problem* p, int nrhs, const double* x, double* y, int flags);
@@ -140,10 +203,13 @@ aifmm_status aifmm_total_field(aifmm_problem* p, int nrhs, const double* theta, 
  * (which: 0 incoming check, 1 incoming charge, 2 outgoing check, 3 outgoing charge). */
 aifmm_status aifmm_level_ranks(aifmm_problem* p, int level, int* rank_in, int* rank_out);
 aifmm_status aifmm_box_skeleton(aifmm_problem* p, int level, int box, int which, int* out, int cap, int* count);
-/* Wall time of the last phases in ms: [0] build_tree [1] tables [2] assemble [3] factorize_solve. */
+/* Wall time of the last phases in ms: [0] build_tree [1] tables [2] assemble [3] factorize_solve
+ * [4] factorize [5] solve (6 values). */
 aifmm_status aifmm_phase_times(const aifmm_problem* p, double* ms);
 /* Number of kernel launches issued by the last factorize_solve and by the last assemble. */
 aifmm_status aifmm_launch_counts(const aifmm_problem* p, long* factor_solve, long* assemble);
+/* Number of kernel launches issued by the last factorize and by the last solve. */
+aifmm_status aifmm_launch_counts_split(const aifmm_problem* p, long* factorize, long* solve);
 /* CUDA-event timing of one kind of kernel launch (0 QR factorisation, 1 QR solve,
  * 2 GEMM) on the handle's stream while enabled; reading returns the launches, the
  * summed device time (ms) and the summed algorithmic flops since it was enabled. */
@@ -156,10 +222,48 @@ aifmm_status aifmm_kernel_profile_read(aifmm_problem* p, int kind, long* launche
  * [9] ms in the ACA (launch to ranks on the host), [10] ms for the interpolative
  * operators, [11] ms for the M2L and P2P block entries, [12] ms of ACA kernel time
  * (CUDA events); device memory held by the handle: [13] bytes of the block pool, [14] bytes
- * of the assembly's reusable workspaces.  n <= 15 values are written. */
+ * of its workspaces (the assembly's reusable buffers, per-step scratch, descriptor
+ * ring).  n <= 15 values are written. */
 aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n);
 /* The CUDA stream the handle works on (cudaStream_t). */
 aifmm_status aifmm_get_stream(const aifmm_problem* p, void** stream);
+
+/* ---- Serving loop (no counterpart in the reference, which solves one problem with
+ * one right-hand side per process run, testFMM2D_find_error.cpp:41-176).
+ * Factorisations stay resident on the device under a caller-chosen key; solve
+ * requests against a key are batched continuously (every solve queued for a key
+ * when a worker takes it runs as one multi-RHS aifmm_solve); factorisations are
+ * admitted by device footprint and the least recently used idle one is evicted to
+ * make room (a later solve on an evicted key factors it again).  Workers drive
+ * their own handles and streams, so different keys overlap on the GPU.  All calls
+ * are thread-safe. */
+typedef struct aifmm_server aifmm_server;
+/* hbm_budget_bytes <= 0: 80% of the device memory free at creation.  workers: host
+ * threads (each runs one request at a time).  max_batch_rhs: right-hand sides per
+ * batched solve (and the largest nrhs of one request). */
+aifmm_status aifmm_server_create(int device, double hbm_budget_bytes, int workers, int max_batch_rhs,
+                                 aifmm_server** out);
+/* Runs the queued requests to completion, then stops the workers and frees every factor. */
+aifmm_status aifmm_server_destroy(aifmm_server* s);
+/* Queue a factorisation of desc under key (tables with the 6-digit round trip, tree,
+ * assembly, FP64 factorisation); replaces an earlier one under the same key. */
+aifmm_status aifmm_server_factorize(aifmm_server* s, long long key, const aifmm_desc* desc, long* request);
+/* Queue nrhs right-hand sides against key (which must have been submitted for
+ * factorisation).  b and x: host memory, N x nrhs complex, column-major; both must
+ * stay valid until the request is waited for. */
+aifmm_status aifmm_server_solve(aifmm_server* s, long long key, int nrhs, const double* b, double* x,
+                                long* request);
+/* Wait up to timeout_s seconds for a request.  AIFMM_ERR_STATE: not finished yet (wait
+ * again).  Otherwise *result is the request's status, *latency_ms the time from
+ * submission to completion and *batch_rhs the right-hand sides of the batch a solve
+ * ran in (any output pointer may be NULL); the request is then forgotten. */
+aifmm_status aifmm_server_wait(aifmm_server* s, long request, double timeout_s, aifmm_status* result,
+                               double* latency_ms, int* batch_rhs);
+/* [0] p50 and [1] p99 solve latency (ms), [2] p50 and [3] p99 factorisation latency,
+ * [4] solves and [5] factorisations completed, [6] evictions, [7] solve batches,
+ * [8] mean right-hand sides per batch, [9] device bytes held by factors, [10] resident
+ * factorisations, [11] failed requests.  n <= 12 values are written. */
+aifmm_status aifmm_server_stats(aifmm_server* s, double* out, int n);
 
 #ifdef __cplusplus
 }

@@ -155,18 +155,27 @@ class FMM2DTree {
   void assemble_M2L() {}
   void initialise_phase() {}
   void initialise_P2P_Leaf_Level() {}
-  // eliminate_phase_efficient + back_substitution_phase with the right-hand sides carried
+  // eliminate_phase_efficient (F:2407-2451) with the base-level factorisation; the
+  // reference carries the right-hand side through it, here the factors are kept and
+  // the right-hand side goes through back_substitution_phase
   void eliminate_phase_efficient() {
-    check(aifmm_factorize_solve(K_->handle(), nrhs_, reinterpret_cast<const double*>(b_.data()),
-                                reinterpret_cast<double*>(x_.data()), AIFMM_PTR_HOST), K_->handle());
+    check(aifmm_factorize(K_->handle(), AIFMM_PRECISION_FP64, 0), K_->handle());
   }
-  void back_substitution_phase() {}
+  // the right-hand-side updates of the elimination, the base-level solve and the
+  // back substitution (F:1968-2001, 2252-2293, 2453-2532) with the kept factors
+  void back_substitution_phase() {
+    check(aifmm_solve(K_->handle(), nrhs_, reinterpret_cast<const double*>(b_.data()), N_,
+                      reinterpret_cast<double*>(x_.data()), N_, nullptr, AIFMM_PTR_HOST), K_->handle());
+  }
+  // another right-hand side against the same factors
+  void set_rhs(const dtype* properties) { b_.assign(properties, properties + (size_t)N_ * nrhs_); }
   const std::vector<dtype>& solution() const { return x_; }
   // error_check (F:2534-2581): relative forward error against x_true
   double error_check(const std::vector<dtype>& x_true) const {
-    double e = 0.0, n = 0.0;
-    for (size_t i = 0; i < x_.size(); ++i) { e += std::norm(x_[i] - x_true[i]); n += std::norm(x_true[i]); }
-    return std::sqrt(e / n);
+    double rel = 0.0;
+    check(aifmm_find_error(K_->handle(), nrhs_, reinterpret_cast<const double*>(x_.data()), N_,
+                           reinterpret_cast<const double*>(x_true.data()), N_, &rel, AIFMM_PTR_HOST), K_->handle());
+    return rel;
   }
 
  private:
