@@ -23,7 +23,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "lib", "libaifmm_b200.so")
 _lib = None
 
-PTR_HOST, PTR_DEVICE, KEEP_ASSEMBLY = 0, 1, 2
+PTR_HOST, PTR_DEVICE, KEEP_ASSEMBLY, SOLVE_GRAPH = 0, 1, 2, 4
 PRECISION_FP64 = 0
 Q_KINDS = {"gaussian160": 0, "multi_gauss": 1, "plasma": 2, "flatbump": 3, "cavity": 4, "lens": 5,
            "gauss_aw": 10, "disk": 11}
@@ -72,6 +72,7 @@ SIGNATURES = {
                      _d, ctypes.c_int, _d, _d, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "aifmm_trim": ([_v], ctypes.c_int),
     "aifmm_set_factor_tolerance": ([_v, ctypes.c_int], ctypes.c_int),
+    "aifmm_autotune": ([_v, _d, _i], ctypes.c_int),
     "aifmm_compressed_matvec": ([_v, ctypes.c_int, _d, ctypes.c_long, _d, ctypes.c_long, ctypes.c_int], ctypes.c_int),
     "aifmm_solve_refined": ([_v, ctypes.c_int, _d, ctypes.c_long, _d, ctypes.c_long, ctypes.c_double, ctypes.c_int,
                              _i, _d, ctypes.c_int], ctypes.c_int),
@@ -219,6 +220,13 @@ class LSKernel:
     def getCol(self, k, rows):
         return self.getMatrix(rows, [k])[:, 0]
 
+    def autotune(self):
+        """time both GEMM tile widths on this problem's shapes; returns (timings ms, chosen widths)"""
+        ms = np.zeros(4)
+        tc = np.zeros(2, dtype=np.int32)
+        self._ck(load().aifmm_autotune(self.h, _dp(ms), _ip(tc)))
+        return ms, tc
+
     def zgemm(self, A, B, C=None, alpha=1.0, beta=0.0, opA=0, opB=0):
         """C = alpha op(A) op(B) + beta C with the solver's batched GEMM kernel (op 1 = conjugate transpose)."""
         A = np.asfortranarray(A, dtype=np.complex128)
@@ -325,12 +333,14 @@ class FMM2DTree:
         return x, it.value, rr.value
 
     # the right-hand-side half with kept factors (F:1968-2001, 2252-2293, 2453-2532)
-    def solve_factored(self, b):
+    def solve_factored(self, b, graph=False):
+        """x for right-hand sides b (nrhs, N) with the kept factors; graph=True replays the
+        CUDA graph of this right-hand-side count (recorded by the first such solve)."""
         b = np.ascontiguousarray(np.atleast_2d(np.asarray(b, np.complex128)))
         x = np.zeros_like(b)
         N = self.K.N
         self._ck(load().aifmm_solve(self.K.h, b.shape[0], _dp(b.view(np.float64)), N, _dp(x.view(np.float64)), N,
-                                    None, PTR_HOST))
+                                    None, PTR_HOST | (SOLVE_GRAPH if graph else 0)))
         self.x = x
         return x
 

@@ -685,15 +685,22 @@ __global__ void __launch_bounds__(kT) formq_kernel(const FormQJob* __restrict__ 
 // into registers before the current chunk is multiplied out of shared memory,
 // so one load latency hides behind each chunk's arithmetic.  Accumulation runs
 // over k in increasing order, term after term.
-constexpr int TM = 32, TN = 32, TK = 32;
+// Output tile TM x TN(SJ) with TN = 16 SJ: SJ = 2 gives 32 x 32 tiles, SJ = 1
+// gives 32 x 16 tiles for thin products (a block times a few right-hand sides).
+constexpr int TM = 32, TK = 32;
+template <int SJ>
 __device__ __forceinline__ void gemm_fetch(const GemmTerm& T, int k0, int row0, int col0, int m, int n,
-                                           double2 (&ra)[4], double2 (&rb)[4]) {
+                                           double2 (&ra)[4], double2 (&rb)[2 * SJ]) {
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
     const int e = threadIdx.x + 256 * u;
     const int kk = e / TM, ii = e % TM, gi = row0 + ii, gk = k0 + kk;
     ra[u] = make_double2(0.0, 0.0);
     if (gi < m && gk < T.k) ra[u] = T.opA ? cconj(T.A[gk + (size_t)gi * T.lda]) : T.A[gi + (size_t)gk * T.lda];
+  }
+#pragma unroll
+  for (int u = 0; u < 2 * SJ; ++u) {
+    const int e = threadIdx.x + 256 * u;
     const int jj = e / TK, kb = e % TK, gj = col0 + jj, gkb = k0 + kb;
     rb[u] = make_double2(0.0, 0.0);
     if (gj < n && gkb < T.k) rb[u] = T.opB ? cconj(T.B[gj + (size_t)gkb * T.ldb]) : T.B[gkb + (size_t)gj * T.ldb];
@@ -703,11 +710,13 @@ __device__ __forceinline__ void gemm_fetch(const GemmTerm& T, int k0, int row0, 
 // one B element, two accumulators)
 __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
   asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-               : "+d"(d[0]), "+d"(d[1])
-               : "d"(a), "d"(b));
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
 }
+template <int SJ>
 __global__ void __launch_bounds__(256) gemm_kernel(const GemmDesc* __restrict__ ds, const GemmTerm* __restrict__ terms,
                                                    const int* __restrict__ tile_off, int nd) {
+  constexpr int TN = 16 * SJ;
   const int bid = blockIdx.x;
   int lo = 0, hi = nd - 1;
   while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (tile_off[mid] <= bid) lo = mid; else hi = mid - 1; }
@@ -718,20 +727,26 @@ __global__ void __launch_bounds__(256) gemm_kernel(const GemmDesc* __restrict__ 
   __shared__ double2 As[TK][TM + 1];
   __shared__ double2 Bs[TK][TN + 1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int si = warp & 3, sj0 = 2 * (warp >> 2);
-  double cr[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, ci[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+  const int si = warp & 3, sj0 = SJ * (warp >> 2);
+  double cr[SJ][2], ci[SJ][2];
+#pragma unroll
+  for (int q = 0; q < SJ; ++q) cr[q][0] = cr[q][1] = ci[q][0] = ci[q][1] = 0.0;
   const int row0 = tm * TM, col0 = tn * TN;
   int tt = 0, k0 = 0;
   GemmTerm T{};
   bool have = false;
   for (; tt < D.nterms; ++tt) { T = terms[D.term0 + tt]; if (T.k > 0) { have = true; break; } }
-  double2 ra[4], rb[4];
-  if (have) gemm_fetch(T, k0, row0, col0, D.m, D.n, ra, rb);
+  double2 ra[4], rb[2 * SJ];
+  if (have) gemm_fetch<SJ>(T, k0, row0, col0, D.m, D.n, ra, rb);
   while (have) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int e = threadIdx.x + 256 * u;
       As[e / TM][e % TM] = ra[u];
+    }
+#pragma unroll
+    for (int u = 0; u < 2 * SJ; ++u) {
+      const int e = threadIdx.x + 256 * u;
       Bs[e % TK][e / TK] = rb[u];
     }
     __syncthreads();
@@ -743,10 +758,10 @@ __global__ void __launch_bounds__(256) gemm_kernel(const GemmDesc* __restrict__ 
       k0 = 0;
       for (++tt; tt < D.nterms; ++tt) { T = terms[D.term0 + tt]; if (T.k > 0) { next = true; break; } }
     }
-    if (next) gemm_fetch(T, k0, row0, col0, D.m, D.n, ra, rb);
+    if (next) gemm_fetch<SJ>(T, k0, row0, col0, D.m, D.n, ra, rb);
     // FP64 tensor cores: mma.sync m8n8k4 (DMMA).  Warp w owns the 8x8 output
-    // sub-tiles (si, sj0) and (si, sj0 + 1) of the 32x32 tile; a complex product
-    // is four real products, Cr += Ar Br + (-Ai) Bi and Ci += Ar Bi + Ai Br.
+    // sub-tiles (si, sj0 .. sj0 + SJ - 1) of the tile; a complex product is four
+    // real products, Cr += Ar Br + (-Ai) Bi and Ci += Ar Bi + Ai Br.
     // Fragments (PTX ISA, mma.m8n8k4 .f64): A row = lane/4, col = lane%4;
     // B row = lane%4, col = lane/4; C row = lane/4, cols 2(lane%4) + {0, 1}.
 #pragma unroll
@@ -754,7 +769,7 @@ __global__ void __launch_bounds__(256) gemm_kernel(const GemmDesc* __restrict__ 
       const double2 a = As[k4 + (lane & 3)][si * 8 + (lane >> 2)];
       const double ar = a.x, ai = a.y, nai = -a.y;
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
+      for (int q = 0; q < SJ; ++q) {
         const double2 b = Bs[k4 + (lane & 3)][(sj0 + q) * 8 + (lane >> 2)];
         dmma884(cr[q], ar, b.x);
         dmma884(cr[q], nai, b.y);
@@ -767,7 +782,7 @@ __global__ void __launch_bounds__(256) gemm_kernel(const GemmDesc* __restrict__ 
   }
   const bool zero_beta = D.beta.x == 0.0 && D.beta.y == 0.0;
 #pragma unroll
-  for (int q = 0; q < 2; ++q)
+  for (int q = 0; q < SJ; ++q)
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int gi = row0 + si * 8 + (lane >> 2), gj = col0 + (sj0 + q) * 8 + 2 * (lane & 3) + h;
@@ -955,9 +970,10 @@ int aifmm_launch_formq(const FormQJob* d_jobs, const int* d_col_off, int njobs, 
   return (int)cudaGetLastError();
 }
 int aifmm_launch_gemm(const GemmDesc* d, const GemmTerm* d_terms, const int* d_tile_off, int nd, int total_tiles,
-                      cudaStream_t s) {
+                      cudaStream_t s, int tile_cols) {
   if (nd <= 0 || total_tiles <= 0) return 0;
-  gemm_kernel<<<total_tiles, 256, 0, s>>>(d, d_terms, d_tile_off, nd);
+  if (tile_cols == 16) gemm_kernel<1><<<total_tiles, 256, 0, s>>>(d, d_terms, d_tile_off, nd);
+  else gemm_kernel<2><<<total_tiles, 256, 0, s>>>(d, d_terms, d_tile_off, nd);
   return (int)cudaGetLastError();
 }
 int aifmm_launch_geam(const GeamDesc* d, const long long* d_off, int nd, long long total, cudaStream_t s) {

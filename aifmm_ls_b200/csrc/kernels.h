@@ -141,8 +141,9 @@ int aifmm_launch_qr_factor_smem(const QRJob* d_jobs, int njobs, size_t smem, cud
 size_t aifmm_compress_smem_bytes(int m, int rK, int c, int rb);
 int aifmm_launch_compress_p2p(const CompressJob* d_jobs, int njobs, size_t smem, cudaStream_t s);
 int aifmm_launch_formq(const FormQJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s);
+// tile_cols: output tile width, 32 (32 x 32 tiles) or 16 (32 x 16 tiles for thin products)
 int aifmm_launch_gemm(const GemmDesc* d, const GemmTerm* d_terms, const int* d_tile_off, int nd, int total_tiles,
-                      cudaStream_t s);
+                      cudaStream_t s, int tile_cols);
 int aifmm_launch_geam(const GeamDesc* d, const long long* d_off, int nd, long long total, cudaStream_t s);
 int aifmm_launch_norms(const NormDesc* d, int nd, cudaStream_t s);
 int aifmm_launch_skel_lu(const SkelLUJob* d, int nd, const EntryCtx& ctx, cudaStream_t s);

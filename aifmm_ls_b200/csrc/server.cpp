@@ -159,6 +159,7 @@ struct aifmm_server {
     if ((st = aifmm_tables_compute(p, 1)) != AIFMM_OK) return fail(st);
     if ((st = aifmm_build_tree(p)) != AIFMM_OK) return fail(st);
     if ((st = aifmm_assemble(p)) != AIFMM_OK) return fail(st);
+    if ((st = aifmm_autotune(p, nullptr, nullptr)) != AIFMM_OK) return fail(st);  // tile widths for this problem
     if ((st = aifmm_factorize(p, AIFMM_PRECISION_FP64, 0)) != AIFMM_OK) return fail(st);
     if ((st = aifmm_trim(p)) != AIFMM_OK) return fail(st);
     double v[15] = {0};

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -437,6 +438,39 @@ struct aifmm_problem {
     f = QRF();
   }
 
+  // ------------------------------------------------------------------ recording
+  // While a solve plan is recorded, descriptor arrays go to device blocks owned
+  // by the plan (not the staging ring, whose slots are reused) and every launch
+  // is also kept as a closure, to be captured into a CUDA graph afterwards.
+  bool recording = false;
+  std::vector<std::function<int(cudaStream_t)>> rec_ops;
+  std::vector<std::pair<void*, size_t>> rec_dev;     // descriptor blocks of the plan being recorded
+  std::vector<std::vector<char>> rec_host;           // their host sources, kept until the uploads finish
+  std::vector<const void*> put_many_(std::initializer_list<std::pair<const void*, size_t>> parts) {
+    if (!recording) return stage.put_many(parts, cur);
+    size_t tot = 0;
+    for (auto& pr : parts) tot += (pr.second + 255) & ~size_t(255);
+    const size_t bytes = std::max<size_t>(tot, 256);
+    char* d = static_cast<char*>(pool.alloc(bytes));
+    rec_dev.push_back({d, bytes});
+    rec_host.emplace_back(tot);
+    std::vector<char>& h = rec_host.back();
+    std::vector<const void*> out;
+    size_t o = 0;
+    for (auto& pr : parts) {
+      memcpy(h.data() + o, pr.first, pr.second);
+      out.push_back(d + o);
+      o += (pr.second + 255) & ~size_t(255);
+    }
+    CK(cudaMemcpyAsync(d, h.data(), tot, cudaMemcpyHostToDevice, cur));
+    return out;
+  }
+  int run_op(std::function<int(cudaStream_t)> f) {
+    const int e = f(cur);
+    if (recording) rec_ops.push_back(std::move(f));
+    return e;
+  }
+
   // ------------------------------------------------------------------ batches
   std::vector<GemmDesc> gd; std::vector<GemmTerm> gt;
   std::vector<GeamDesc> ged;
@@ -479,21 +513,33 @@ struct aifmm_problem {
     }
     gd.push_back(g);
   }
+  // GEMM output-tile width per product shape, set by autotune(): [0] for batches
+  // whose products are all thin (n <= 16 columns, e.g. a block times the
+  // right-hand sides), [1] otherwise
+  int gemm_cols[2] = {32, 32};
   void flush_gemm() {
     if (gd.empty()) { gt.clear(); return; }
+    int nmax = 0;
+    for (auto& g : gd) nmax = std::max(nmax, g.n);
+    const int tc = gemm_cols[nmax <= 16 ? 0 : 1];
     std::vector<int> off(gd.size());
     int tot = 0;
-    for (size_t i = 0; i < gd.size(); ++i) { off[i] = tot; tot += ((gd[i].m + 31) / 32) * ((gd[i].n + 31) / 32); }
+    for (size_t i = 0; i < gd.size(); ++i) { off[i] = tot; tot += ((gd[i].m + 31) / 32) * ((gd[i].n + tc - 1) / tc); }
     double fl = 0;
     for (auto& g : gd)
       for (int t = 0; t < g.nterms; ++t) fl += 8.0 * g.m * g.n * gt[g.term0 + t].k;
     if (gt.empty()) gt.push_back(GemmTerm{});
-    auto ptrs = stage.put_many({{gt.data(), gt.size() * sizeof(GemmTerm)}, {gd.data(), gd.size() * sizeof(GemmDesc)},
-                                {off.data(), off.size() * sizeof(int)}}, cur);
+    auto ptrs = put_many_({{gt.data(), gt.size() * sizeof(GemmTerm)}, {gd.data(), gd.size() * sizeof(GemmDesc)},
+                           {off.data(), off.size() * sizeof(int)}});
     cudaEvent_t a;
     const bool pr = prof_begin(2, a);
-    KL(aifmm_launch_gemm(static_cast<const GemmDesc*>(ptrs[1]), static_cast<const GemmTerm*>(ptrs[0]),
-                         static_cast<const int*>(ptrs[2]), (int)gd.size(), tot, cur));
+    {
+      const GemmDesc* d1 = static_cast<const GemmDesc*>(ptrs[1]);
+      const GemmTerm* d0 = static_cast<const GemmTerm*>(ptrs[0]);
+      const int* d2 = static_cast<const int*>(ptrs[2]);
+      const int nd = (int)gd.size();
+      KL(run_op([=](cudaStream_t s_) { return aifmm_launch_gemm(d1, d0, d2, nd, tot, s_, tc); }));
+    }
     if (pr) prof_end(2, a, fl);
     gd.clear(); gt.clear();
   }
@@ -511,15 +557,28 @@ struct aifmm_problem {
     std::vector<long long> off(ged.size());
     long long tot = 0;
     for (size_t i = 0; i < ged.size(); ++i) { off[i] = tot; tot += (long long)ged[i].m * ged[i].n; }
-    auto ptrs = stage.put_many({{ged.data(), ged.size() * sizeof(GeamDesc)}, {off.data(), off.size() * sizeof(long long)}}, cur);
-    KL(aifmm_launch_geam(static_cast<const GeamDesc*>(ptrs[0]), static_cast<const long long*>(ptrs[1]),
-                         (int)ged.size(), tot, cur));
+    auto ptrs = put_many_({{ged.data(), ged.size() * sizeof(GeamDesc)}, {off.data(), off.size() * sizeof(long long)}});
+    {
+      const GeamDesc* d0 = static_cast<const GeamDesc*>(ptrs[0]);
+      const long long* d1 = static_cast<const long long*>(ptrs[1]);
+      const int nd = (int)ged.size();
+      KL(run_op([=](cudaStream_t s_) { return aifmm_launch_geam(d0, d1, nd, tot, s_); }));
+    }
     ged.clear();
   }
   void zero(const Blk& b) {
     if (b.size() == 0) return;
-    if (b.ld == b.r) CK(cudaMemsetAsync(b.p, 0, sizeof(double2) * (size_t)b.r * b.c, cur));
-    else for (int j = 0; j < b.c; ++j) CK(cudaMemsetAsync(b.p + (size_t)j * b.ld, 0, sizeof(double2) * b.r, cur));
+    if (b.ld == b.r) {
+      double2* p_ = b.p;
+      const size_t n_ = sizeof(double2) * (size_t)b.r * b.c;
+      CK((cudaError_t)run_op([=](cudaStream_t s_) { return (int)cudaMemsetAsync(p_, 0, n_, s_); }));
+    } else {
+      for (int j = 0; j < b.c; ++j) {
+        double2* p_ = b.p + (size_t)j * b.ld;
+        const size_t n_ = sizeof(double2) * b.r;
+        CK((cudaError_t)run_op([=](cudaStream_t s_) { return (int)cudaMemsetAsync(p_, 0, n_, s_); }));
+      }
+    }
   }
   // QR factorisation of A in place (threshold 0 -> Eigen default)
   void qr_prepare(QRF& f, const Blk& A, double thr, bool persistent) {
@@ -611,13 +670,17 @@ struct aifmm_problem {
       std::vector<int> off(small.size());
       int tot = 0;
       for (size_t i = 0; i < small.size(); ++i) { off[i] = tot; tot += (small[i].nrhs + 7) / 8; }
-      auto ptrs = stage.put_many({{small.data(), small.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}}, cur);
+      auto ptrs = put_many_({{small.data(), small.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}});
       double fl = 0;
       for (auto& j : small) { const double mz = std::min(j.m, j.n); fl += (16.0 * j.m * mz - 4.0 * mz * mz) * j.nrhs; }
       cudaEvent_t a;
       const bool pr = prof_begin(1, a);
-      KL(aifmm_launch_qr_solve_warp(static_cast<const SolveJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]),
-                                    (int)small.size(), tot, mmax, nmax, cur));
+      {
+        const SolveJob* d0 = static_cast<const SolveJob*>(ptrs[0]);
+        const int* d1 = static_cast<const int*>(ptrs[1]);
+        const int nj = (int)small.size();
+        KL(run_op([=](cudaStream_t s_) { return aifmm_launch_qr_solve_warp(d0, d1, nj, tot, mmax, nmax, s_); }));
+      }
       if (pr) prof_end(1, a, fl);
     }
     if (!large.empty()) {
@@ -628,13 +691,17 @@ struct aifmm_problem {
         tot += large[i].nrhs;
         large[i].work = static_cast<double2*>(scratch.get(sizeof(double2) * (size_t)large[i].m * large[i].nrhs));
       }
-      auto ptrs = stage.put_many({{large.data(), large.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}}, cur);
+      auto ptrs = put_many_({{large.data(), large.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}});
       double fl = 0;
       for (auto& j : large) { const double mz = std::min(j.m, j.n); fl += (16.0 * j.m * mz - 4.0 * mz * mz) * j.nrhs; }
       cudaEvent_t a;
       const bool pr = prof_begin(1, a);
-      KL(aifmm_launch_qr_solve(static_cast<const SolveJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]),
-                               (int)large.size(), tot, cur));
+      {
+        const SolveJob* d0 = static_cast<const SolveJob*>(ptrs[0]);
+        const int* d1 = static_cast<const int*>(ptrs[1]);
+        const int nj = (int)large.size();
+        KL(run_op([=](cudaStream_t s_) { return aifmm_launch_qr_solve(d0, d1, nj, tot, s_); }));
+      }
       if (pr) prof_end(1, a, fl);
     }
     sj.clear();
@@ -775,6 +842,7 @@ struct aifmm_problem {
   void destroy() {
     if (st) cudaStreamSynchronize(st);
     if (st2) cudaStreamSynchronize(st2);
+    release_plans();
     pool.release_all();
     cudaFree(d_pts); cudaFree(d_q); cudaFree(d_leafc); cudaFree(d_leafxy); cudaFree(d_M); cudaFree(d_near);
     cudaFree(d_iota);
@@ -2183,6 +2251,7 @@ struct aifmm_problem {
         B.elim = false;
       }
     release_solve_state();
+    release_plans();
     drop(base_A);
     drop_qrf(base_qr);
     factored = false;
@@ -2244,26 +2313,56 @@ struct aifmm_problem {
     ms_factor = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
 
-  // b and x: N x nrhs complex, column stride ldb / ldx (>= N), host or device
+  // b and x: N x nrhs complex, column stride ldb / ldx (>= N), host or device.
+  // With AIFMM_SOLVE_GRAPH the solve replays the CUDA graph of this right-hand-side
+  // count (recorded by the first such solve after a factorisation).
   void solve_rhs(int nrhs_, const double* b, long ldb, double* x, long ldx, int flags) {
     if (!factored) throw Fail(AIFMM_ERR_STATE, "factorize() must run before solve()");
     if (nrhs_ < 1) throw Fail(AIFMM_ERR_ARG, "nrhs must be positive");
     if (ldb < N || ldx < N) throw Fail(AIFMM_ERR_ARG, "leading dimension smaller than the number of unknowns");
     auto t0 = std::chrono::steady_clock::now();
     const long l0 = launches_;
-    nrhs = nrhs_;
     const bool dev = flags & AIFMM_PTR_DEVICE;
-    const size_t bytes = sizeof(double2) * (size_t)N * nrhs;
-    Tmp tb(this, dev ? 1 : bytes), tx(this, dev ? 1 : bytes);
-    const double2* db = reinterpret_cast<const double2*>(b);
-    long ldd_b = ldb;
-    if (!dev) {
-      CK(cudaMemcpy2DAsync(tb.ptr, sizeof(double2) * N, b, sizeof(double2) * ldb, sizeof(double2) * N, nrhs,
-                           cudaMemcpyHostToDevice, st));
-      db = tb.as<double2>();
-      ldd_b = N;
+    const cudaMemcpyKind h2d = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind d2h_ = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (flags & AIFMM_SOLVE_GRAPH) {
+      SolvePlan& pl = plan_for(nrhs_);
+      CK(cudaMemcpy2DAsync(pl.bin, sizeof(double2) * N, b, sizeof(double2) * ldb, sizeof(double2) * N, nrhs_, h2d, st));
+      CK(cudaGraphLaunch(pl.exec, st));
+      CK(cudaMemcpy2DAsync(x, sizeof(double2) * ldx, pl.xout, sizeof(double2) * N, sizeof(double2) * N, nrhs_, d2h_, st));
+      sync();
+      launches_ += pl.launches;
+    } else {
+      const size_t bytes = sizeof(double2) * (size_t)N * nrhs_;
+      Tmp tb(this, dev ? 1 : bytes), tx(this, dev ? 1 : bytes);
+      const double2* db = reinterpret_cast<const double2*>(b);
+      double2* dx = reinterpret_cast<double2*>(x);
+      long lb = ldb, lx = ldx;
+      if (!dev) {
+        CK(cudaMemcpy2DAsync(tb.ptr, sizeof(double2) * N, b, sizeof(double2) * ldb, sizeof(double2) * N, nrhs_,
+                             cudaMemcpyHostToDevice, st));
+        db = tb.as<double2>();
+        dx = tx.as<double2>();
+        lb = lx = N;
+      }
+      solve_core(nrhs_, db, lb, dx, lx);
+      if (!dev)
+        CK(cudaMemcpy2DAsync(x, sizeof(double2) * ldx, dx, sizeof(double2) * N, sizeof(double2) * N, nrhs_,
+                             cudaMemcpyDeviceToHost, st));
+      sync();
+      release_solve_state();
     }
-    // per-solve blocks: every box's rhs, sxb, sy, smr
+    prof_collect();
+    pool.commit_frees();
+    launches_solve = launches_ - l0;
+    ms_solve = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+
+  // The solve on device buffers (the per-solve blocks stay in the boxes until
+  // release_solve_state or a plan takes them).
+  void solve_core(int nrhs_, const double2* db, long ldd_b, double2* dx, long ldd_x) {
+    nrhs = nrhs_;
+    cur = st;
     release_solve_state();
     for (int j = 2; j <= depth; ++j)
       for (int k = 0; k < nBoxes[j]; ++k) {
@@ -2302,8 +2401,6 @@ struct aifmm_problem {
     for (int j = 2; j <= depth; ++j)
       for (const auto& ks : bwd_waves[j]) backward_wave(j, ks);
     // gather the leaf particles
-    double2* dx = dev ? reinterpret_cast<double2*>(x) : tx.as<double2>();
-    const long ldd_x = dev ? ldx : N;
     for (int k = 0; k < nBoxes[depth]; ++k) {
       const Blk& px = T[depth][k].particles;
       Blk dst{dx + (size_t)k * rank, rank, nrhs, (int)ldd_x};
@@ -2312,15 +2409,138 @@ struct aifmm_problem {
       if ((int)ged.size() > 20000) flush_geam();
     }
     flush_geam();
-    if (!dev)
-      CK(cudaMemcpy2DAsync(x, sizeof(double2) * ldx, dx, sizeof(double2) * N, sizeof(double2) * N, nrhs,
-                           cudaMemcpyDeviceToHost, st));
+  }
+
+  // ---- autotuner: the GEMM tile width per product shape, from timings of both
+  // widths on batches shaped like this problem's products (leaf blocks rank x rank,
+  // their products with 8 right-hand sides, and the 4-rank blocks of the level
+  // above), CUDA events on the handle's stream; the faster width is kept per shape.
+  double tune_ms[2][2] = {{0, 0}, {0, 0}};  // [thin, wide][16, 32]
+  void autotune() {
+    const int r = rank, R = std::min(4 * rank, 160);
+    const int nb = std::max(256, std::min(4096, nBoxes[depth] / 2));
+    struct Shape { int m, n, k; };
+    const Shape thin[2] = {{r, 8, r}, {R, 8, R}}, wide[2] = {{r, r, r}, {R, R, R}};
+    size_t elems = 0;
+    for (const Shape* sh : {thin, wide})
+      for (int q = 0; q < 2; ++q) elems = std::max(elems, (size_t)sh[q].m * sh[q].k + (size_t)sh[q].k * sh[q].n +
+                                                              (size_t)sh[q].m * sh[q].n);
+    Tmp buf(this, sizeof(double2) * elems * nb);
+    CK(cudaMemsetAsync(buf.ptr, 0, sizeof(double2) * elems * nb, st));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int bucket = 0; bucket < 2; ++bucket) {
+      const Shape* sh = bucket == 0 ? thin : wide;
+      for (int v = 0; v < 2; ++v) {
+        gemm_cols[bucket] = v == 0 ? 16 : 32;
+        float best = 1e30f;
+        for (int rep_ = 0; rep_ < 6; ++rep_) {
+          for (int j = 0; j < nb; ++j) {
+            const Shape& z = sh[j & 1];
+            double2* base = buf.as<double2>() + elems * j;
+            Blk A{base, z.m, z.k, z.m}, B{base + (size_t)z.m * z.k, z.k, z.n, z.k};
+            Blk C{base + (size_t)z.m * z.k + (size_t)z.k * z.n, z.m, z.n, z.m};
+            gemm(C, A, 0, B, 0, C1, C1);
+          }
+          cur = st;
+          CK(cudaEventRecord(e0, st));
+          flush_gemm();
+          CK(cudaEventRecord(e1, st));
+          CK(cudaEventSynchronize(e1));
+          float ms_ = 0.f;
+          CK(cudaEventElapsedTime(&ms_, e0, e1));
+          if (rep_ > 0) best = std::min(best, ms_);  // the first run warms up
+        }
+        tune_ms[bucket][v] = best;
+      }
+      gemm_cols[bucket] = tune_ms[bucket][0] < tune_ms[bucket][1] ? 16 : 32;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     sync();
-    release_solve_state();
-    prof_collect();
     pool.commit_frees();
-    launches_solve = launches_ - l0;
-    ms_solve = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+
+  // ---- CUDA-graph plans: one per right-hand-side count, valid while the factors are
+  struct SolvePlan {
+    int nrhs = 0;
+    double2* bin = nullptr;   // N x nrhs
+    double2* xout = nullptr;  // N x nrhs
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<std::pair<void*, size_t>> owned;  // pool blocks: descriptors, per-solve state, bin, xout
+    long launches = 0;
+  };
+  std::map<int, SolvePlan> plans;
+  void release_plans() {
+    for (auto& kv : plans) {
+      SolvePlan& pl = kv.second;
+      if (pl.exec) cudaGraphExecDestroy(pl.exec);
+      if (pl.graph) cudaGraphDestroy(pl.graph);
+      for (auto& o : pl.owned) pool.defer_free(o.first, o.second);
+    }
+    plans.clear();
+  }
+  SolvePlan& plan_for(int nr) {
+    auto it = plans.find(nr);
+    if (it != plans.end()) return it->second;
+    SolvePlan pl;
+    pl.nrhs = nr;
+    const size_t vb = sizeof(double2) * (size_t)N * nr;
+    pl.bin = static_cast<double2*>(pool.alloc(vb));
+    pl.xout = static_cast<double2*>(pool.alloc(vb));
+    pl.owned.push_back({pl.bin, vb});
+    pl.owned.push_back({pl.xout, vb});
+    CK(cudaMemsetAsync(pl.bin, 0, vb, st));
+    // record: one eager solve whose descriptors go to plan-owned device blocks
+    rec_ops.clear();
+    rec_dev.clear();
+    rec_host.clear();
+    recording = true;
+    const long l0 = launches_;
+    try {
+      solve_core(nr, pl.bin, N, pl.xout, N);
+    } catch (...) {
+      recording = false;
+      throw;
+    }
+    recording = false;
+    sync();
+    rec_host.clear();
+    pl.launches = launches_ - l0;
+    for (auto& d : rec_dev) pl.owned.push_back(d);
+    rec_dev.clear();
+    // the per-solve blocks now belong to the plan (its graph addresses them)
+    for (auto& lv : T)
+      for (auto& B : lv) {
+        for (Blk* b : {&B.sr, &B.sxb, &B.sy, &B.smr, &B.particles, &B.locals, &B.multipoles}) {
+          if (b->p && b->cap) pl.owned.push_back({b->p, b->cap});
+          *b = Blk();
+        }
+      }
+    // capture the recorded launches into a graph
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int err = 0;
+    for (auto& op : rec_ops)
+      if ((err = op(st)) != 0) break;
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    rec_ops.clear();
+    if (err != 0 || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      for (auto& o : pl.owned) pool.defer_free(o.first, o.second);
+      throw Fail(AIFMM_ERR_CUDA, std::string("solve graph capture failed: ") +
+                                     cudaGetErrorString(err ? (cudaError_t)err : ce));
+    }
+    pl.graph = g;
+    const cudaError_t ie = cudaGraphInstantiate(&pl.exec, g, 0);
+    if (ie != cudaSuccess) {
+      cudaGraphDestroy(g);
+      for (auto& o : pl.owned) pool.defer_free(o.first, o.second);
+      throw Fail(AIFMM_ERR_CUDA, std::string("solve graph instantiation failed: ") + cudaGetErrorString(ie));
+    }
+    return plans.emplace(nr, std::move(pl)).first->second;
   }
 
   void factorize_solve(int nrhs_, const double* b, double* x, int flags) {
@@ -2909,6 +3129,15 @@ aifmm_status aifmm_solve(aifmm_problem* p, int nrhs, const double* b, long ldb, 
       CK(cudaEventRecord(p->ev_join, p->st));
       CK(cudaStreamWaitEvent(cs, p->ev_join, 0));
     }
+  });
+}
+
+aifmm_status aifmm_autotune(aifmm_problem* p, double* ms, int* tile_cols) {
+  if (!p) return AIFMM_ERR_ARG;
+  return guard(p, [&] {
+    p->autotune();
+    if (ms) for (int i = 0; i < 4; ++i) ms[i] = p->tune_ms[i / 2][i % 2];
+    if (tile_cols) { tile_cols[0] = p->gemm_cols[0]; tile_cols[1] = p->gemm_cols[1]; }
   });
 }
 

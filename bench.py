@@ -131,6 +131,24 @@ def fp64_peak_tflops(device):
 _TABLES = {}
 
 
+def max_over_ranks(t, pg, device=None):
+    """The slowest rank's time: every rank contributes its own device-timed seconds
+    (NCCL needs the value on the GPU, gloo on the host)."""
+    if pg is None:
+        return t
+    import torch
+    on_gpu = pg.get_backend() == "nccl"
+    tt = torch.tensor([t], dtype=torch.float64, device=f"cuda:{device}" if on_gpu else "cpu")
+    pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def replica_throughput(world_size, unknowns, steps, t_max):
+    """Whole-job unknowns/s of `world_size` independent replicas, each solving
+    `unknowns` per step for `steps` steps, timed as the slowest rank."""
+    return world_size * unknowns * steps / t_max
+
+
 def _oracle_solve_time(O, depth, physics, nrhs, theta_seed):
     """Seconds of one oracle assemble + eliminate + back-substitute (tables precomputed once per depth)."""
     p = O.params(**physics, depth=depth)
@@ -240,6 +258,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer loop (profiling runs)")
     ap.add_argument("--no-serving", action="store_true", help="skip the solve-latency measurement with kept factors")
+    ap.add_argument("--no-peak", action="store_true", help="skip the cuBLAS FP64 peak measurement (profiling runs)")
     ap.add_argument("--batched", type=int, default=1, help="1: also run the 64-problem batched configuration")
     ap.add_argument("--trace", type=float, default=60.0, help="seconds of the serving trace (0: skip)")
     ap.add_argument("--no-kernel-profile", action="store_true",
@@ -301,9 +320,10 @@ def main():
             pg.barrier()
         torch.cuda.synchronize(device)
 
+    tune_ms, tune_cols = K.autotune()
     for _ in range(args.warmup):
         step(False)
-    fp64_peak = fp64_peak_tflops(device) if rank == 0 else None
+    fp64_peak = fp64_peak_tflops(device) if rank == 0 and not args.no_peak else None
     clocks = ClockSampler(device)
     clocks.start()
     barrier()
@@ -323,12 +343,8 @@ def main():
     ev1.record(stream)
     barrier()
     clk = clocks.stop()
-    t_dev = ev0.elapsed_time(ev1) / 1e3
-    if pg is not None:
-        tt = torch.tensor([t_dev], device=f"cuda:{device}")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t_dev = float(tt.item())
-    value = ws * N * args.steps / t_dev
+    t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, pg, device)
+    value = replica_throughput(ws, N, args.steps, t_dev)
     # end to end through the C ABI with host buffers
     t_e2e = None
     if not args.no_e2e:
@@ -340,11 +356,7 @@ def main():
             step(True)
         e1.record(stream)
         barrier()
-        t_e2e = e0.elapsed_time(e1) / 1e3
-        if pg is not None:
-            tt = torch.tensor([t_e2e], device=f"cuda:{device}")
-            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-            t_e2e = float(tt.item())
+        t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, pg, device)
     x = (x_pin if t_e2e is not None else x_dev.cpu()).numpy().view(np.complex128).reshape(NRHS, N)
     finite = bool(np.isfinite(x).all())
     serving = None if args.no_serving else solve_latency(T, K, lib, stream, device, args)
@@ -382,7 +394,7 @@ def main():
                        "parallelism": "replicas" if ws > 1 else "single",
                        "l2": "working set (~17 GiB) far larger than L2; no flush needed"},
             "e2e": None if t_e2e is None else {
-                "value": ws * N * args.steps / t_e2e, "unit": "unknowns/s",
+                "value": replica_throughput(ws, N, args.steps, t_e2e), "unit": "unknowns/s",
                 "h2d_bytes_per_step": int(b_pin.numel() * 8), "d2h_bytes_per_step": int(x_pin.numel() * 8)},
             "gpu_launches": int(launches),
             "phases_ms_per_step": {"assemble": asm_ms / args.steps, "factorize_solve": fs_ms / args.steps,
@@ -390,6 +402,7 @@ def main():
             "solver_stats_last_step": solver_stats,
             "clocks": clk,
             "solution_finite": finite,
+            "gemm_autotune": {"ms_thin16_thin32_wide16_wide32": tune_ms.tolist(), "tile_cols_thin_wide": tune_cols.tolist()},
             "solves_with_cached_factors": serving,
             **extra,
         }

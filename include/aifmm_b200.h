@@ -39,6 +39,12 @@ enum { AIFMM_PTR_HOST = 0, AIFMM_PTR_DEVICE = 1,
         * them otherwise) */
        AIFMM_KEEP_ASSEMBLY = 2 };
 
+/* aifmm_solve: replay a CUDA graph of the whole solve for this right-hand-side count.
+ * The first such solve after a factorisation records the graph (one ordinary solve
+ * plus the capture); the graph, its descriptors and its per-solve buffers stay on the
+ * device until the factors are dropped (build_tree / assemble / factorize / destroy). */
+enum { AIFMM_SOLVE_GRAPH = 4 };
+
 /* Factorisation precision (aifmm_factorize). */
 enum { AIFMM_PRECISION_FP64 = 0 };
 
@@ -142,6 +148,13 @@ aifmm_status aifmm_factorize(aifmm_problem* p, int precision, int flags);
  * the work already queued on it, and work queued on it afterwards sees x. */
 aifmm_status aifmm_solve(aifmm_problem* p, int nrhs, const double* b, long ldb, double* x, long ldx, void* stream,
                          int flags);
+/* No counterpart in the reference: pick the batched GEMM's output-tile width (32 x 16 or
+ * 32 x 32) for this handle by timing both on batches shaped like the problem's products
+ * (thin: blocks times 8 right-hand sides; wide: block times block), at the leaf rank
+ * and at four times it.  ms (may be NULL): 4 timings in ms, [thin 16, thin 32, wide 16,
+ * wide 32]; tile_cols (may be NULL): the chosen widths [thin, wide].  Results do not
+ * depend on the choice beyond rounding: both widths sum every product in the same order. */
+aifmm_status aifmm_autotune(aifmm_problem* p, double* ms, int* tile_cols);
 /* No counterpart in the reference: the recompression tolerance of the next
  * factorisations, 10^-tol_pow (0: the description's tol_pow, which always stays the
  * assembly's ACA tolerance).  A looser factorisation is a cheaper preconditioner for

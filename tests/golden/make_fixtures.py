@@ -1,8 +1,9 @@
 """Generate the golden fixtures in this directory.
 
-Run from the repository root in a container that has the reference checkout:
+Run from the repository root, with the path of a reference checkout
+(vaishna77/AIFMM_LS) as the only argument:
 
-    python tests/golden/make_fixtures.py /root/reference
+    python tests/golden/make_fixtures.py <reference checkout>
 
 Outputs (small JSON files, committed):
   gauss_legendre_10.json   -- the reference's 10-point Gauss-Legendre table
@@ -69,7 +70,9 @@ def bessel_fixture():
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: make_fixtures.py <path of the reference checkout>")
+    ref = sys.argv[1]
     with open(os.path.join(HERE, "gauss_legendre_10.json"), "w") as f:
         json.dump(gl_table(ref), f, indent=1)
     with open(os.path.join(HERE, "interaction_slots.json"), "w") as f:

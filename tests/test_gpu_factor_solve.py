@@ -154,3 +154,22 @@ def test_cli_find_error_protocol(oracle_mod):
     err_o = np.linalg.norm(x - xt) / np.linalg.norm(xt)
     print("find_error protocol: GPU CLI %.3e, oracle %.3e" % (err_gpu, err_o))
     assert 0.5 * err_o <= err_gpu <= 2.0 * err_o + 1e-12
+
+
+def test_graph_solves_equal_eager_solves(table_cache):
+    """AIFMM_SOLVE_GRAPH replays a CUDA graph of the whole solve: the same kernels
+    in the same order as the eager solve, so the same bits; plans are per
+    right-hand-side count and are dropped with the factors."""
+    import aifmm_ls_b200 as A
+    p, tabs = table_cache(depth=4, q_kind="gauss_aw", kappa=40.0, tol_pow=10)
+    K = _kernel(p, tabs)
+    T = A.FMM2DTree(K)
+    for cycle in range(2):
+        T.createTree()
+        T.assemble()
+        T.factorize()
+        for th in ([0.3], [1.0, 2.0, 3.0], [4.4], [5.0, 0.1, 2.2]):
+            b = K.rhs_plane_wave(th)
+            xe = T.solve_factored(b)
+            xg = T.solve_factored(b, graph=True)
+            assert np.array_equal(xe, xg), (cycle, th)

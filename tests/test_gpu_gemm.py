@@ -28,3 +28,18 @@ def test_zgemm_matches_numpy(m, n, k, opA, opB):
     want = alpha * (oa @ ob) + beta * C0
     scale = abs(alpha) * np.abs(oa) @ np.abs(ob) + abs(beta) * np.abs(C0)
     assert np.all(np.abs(C - want) <= 1e-13 * scale + 1e-300), np.max(np.abs(C - want) / scale)
+
+
+def test_autotune_picks_a_width_and_products_stay_exact():
+    import aifmm_ls_b200 as A
+    K = A.LSKernel(depth=4)
+    ms, widths = K.autotune()
+    print("GEMM tile timings (ms) [thin 16, thin 32, wide 16, wide 32]:", ms, "chosen:", widths)
+    assert np.all(ms > 0) and set(widths.tolist()) <= {16, 32}
+    rng = np.random.default_rng(1)
+    for m, n, k in ((36, 8, 36), (144, 144, 144), (37, 3, 70)):
+        Am = rng.standard_normal((m, k)) + 1j * rng.standard_normal((m, k))
+        Bm = rng.standard_normal((k, n)) + 1j * rng.standard_normal((k, n))
+        C = K.zgemm(Am, Bm)
+        scale = np.abs(Am) @ np.abs(Bm)
+        assert np.all(np.abs(C - Am @ Bm) <= 1e-13 * scale)
