@@ -659,6 +659,9 @@ struct Box {
   Mat particle_rhs, multipole_rhs, local_rhs;
   Mat particles, multipoles, locals;
   int rank_in_aca = 0, rank_out_aca = 0;
+  // the L2P_f of neighbour n formed when this box was eliminated, kept for a
+  // solve with new right-hand sides against the same factors (orc_solve_again)
+  Mat Lf[8];
 };
 
 // neighbour numbering of F:11-74 / F:168-1046: 0=(-1,-1) 1=(0,-1) 2=(1,-1)
@@ -1271,6 +1274,7 @@ struct Problem {
         // F:2004-2011
         if (!Nn.Eliminated) Nn.L2P_f = neg(mul(Nn.P2P[k], XL));
         else Nn.L2P_f = neg(mul(Nn.P2L[k], XL));
+        B.Lf[n] = Nn.L2P_f;
         // F:2013-2075
         for (int pI = 0; pI < 8; ++pI) {
           int pp = B.neighbors[pI];
@@ -1318,6 +1322,7 @@ struct Problem {
         Box& Nn = tree[j][nn];
         if (!Nn.Eliminated) Nn.L2P_f = Mat(Nn.P2P[k].r, B.L2P.c);
         else Nn.L2P_f = Mat(Nn.P2L[k].r, B.L2P.c);
+        B.Lf[n] = Nn.L2P_f;
         for (int pI = 0; pI < 8; ++pI) {
           int pp = B.neighbors[pI];
           if (pp == -1) continue;
@@ -1742,6 +1747,63 @@ struct Problem {
     }
   }
 
+  // A solve with new right-hand sides against the factors of the last solve:
+  // the right-hand-side updates that the elimination made box by box
+  // (F:1968, 1997-2001, 2252, 2289-2293), gathered per receiving box.  Box nn
+  // subtracted X[t][nn] QRx^-1 r_nn and L2P_f[t] y_nn from every neighbour t;
+  // those blocks are frozen once nn is eliminated, except L2P_f, kept in Lf.
+  void solve_again() {
+    for (int j = depth; j >= 2; --j) {
+      const int nb = nBoxes[j];
+      std::vector<Mat> xb(nb), y(nb);
+      if (j != depth)
+        for (int k = 0; k < nb; ++k) {
+          int len = 0;
+          for (int c = 0; c < 4; ++c) len += tree[j + 1][4 * k + c].multipole_rhs.r;
+          Mat r(len, nrhs);
+          int o = 0;
+          for (int c = 0; c < 4; ++c) {
+            const Mat& m = tree[j + 1][4 * k + c].multipole_rhs;
+            for (int t = 0; t < nrhs; ++t)
+              for (int x = 0; x < m.r; ++x) r(o + x, t) = m(x, t);
+            o += m.r;
+          }
+          tree[j][k].particle_rhs = r;
+        }
+      for (int k = 0; k < nb; ++k) {
+        Box& B = tree[j][k];
+        for (int n = 0; n < 8; ++n) {
+          const int nn = B.neighbors[n];
+          if (nn == -1 || nn > k) continue;
+          const Box& Nn = tree[j][nn];
+          if (xb[nn].size()) B.particle_rhs = sub(B.particle_rhs, mul(B.P2P[nn], xb[nn]));
+          if (y[nn].size()) B.particle_rhs = sub(B.particle_rhs, mul(Nn.Lf[(n + 4) & 7], y[nn]));
+        }
+        if (B.P2P[k].size() == 0) { xb[k] = Mat(0, nrhs); y[k] = Mat(0, nrhs); continue; }
+        ColPivQR qr(B.P2P[k]);
+        xb[k] = qr.solve(B.particle_rhs);
+        if (B.L2M_f.size() != 0) y[k] = ColPivQR(B.L2M_f).solve(neg(mul(B.P2M, xb[k])));
+        else y[k] = Mat(0, nrhs);
+      }
+      for (int k = 0; k < nb; ++k) {
+        Box& B = tree[j][k];
+        Mat m = y[k];
+        for (int n = 0; n < 8; ++n) {
+          const int nn = B.neighbors[n];
+          if (nn == -1 || nn < k) continue;
+          const Box& Nn = tree[j][nn];
+          if (xb[nn].size() && m.r) m = sub(m, mul(B.P2L[nn], xb[nn]));
+          if (y[nn].size() && m.r) m = sub(m, mul(Nn.Lf[(n + 4) & 7], y[nn]));
+        }
+        B.multipole_rhs = m;
+      }
+    }
+    solve_base(2);
+    for (int j = 2; j <= depth; ++j)
+      for (int k = 0; k < nBoxes[j]; ++k) tree[j][k].Eliminated = true;
+    back_substitution_phase();
+  }
+
   void back_substitution_phase() {  // F:2487-2532
     for (int j = 2; j <= depth; ++j) {
       if (!(schedule & 1)) {
@@ -1980,6 +2042,34 @@ int orc_solve(void* h, int nrhs, const double* b, double* x, double* times) {
       }
   }
   if (times) { times[0] = t1 - t0; times[1] = t2 - t1; times[2] = t3 - t2; times[3] = t4 - t3; }
+  return 0;
+}
+
+// A solve with new right-hand sides against the factors of the last orc_solve.
+int orc_solve_again(void* h, int nrhs, const double* b, double* x) {
+  Problem* P = static_cast<Problem*>(h);
+  P->nrhs = nrhs;
+  const int N = P->N, rank = P->rank;
+  for (int k = 0; k < P->nBoxes[P->depth]; ++k) {
+    Mat r(rank, nrhs);
+    for (int s = 0; s < nrhs; ++s)
+      for (int i = 0; i < rank; ++i) {
+        size_t g = (size_t)s * N + (size_t)k * rank + i;
+        r(i, s) = cd(b[2 * g], b[2 * g + 1]);
+      }
+    P->tree[P->depth][k].particle_rhs = r;
+  }
+  P->solve_again();
+  for (int k = 0; k < P->nBoxes[P->depth]; ++k) {
+    const Mat& px = P->tree[P->depth][k].particles;
+    for (int s = 0; s < nrhs; ++s)
+      for (int i = 0; i < rank; ++i) {
+        size_t g = (size_t)s * N + (size_t)k * rank + i;
+        cd v = i < px.r ? px(i, s) : cd(0, 0);
+        x[2 * g] = v.real();
+        x[2 * g + 1] = v.imag();
+      }
+  }
   return 0;
 }
 

@@ -71,6 +71,8 @@ int orc_total_field(void* h, int nrhs, const double* theta, const double* phi, d
 /* Full pipeline: assemble, eliminate_phase_efficient (with the rhs carried),
  * base solve, back substitution.  times[4] = tree, assemble, factor, solve (s). */
 int orc_solve(void* h, int nrhs, const double* b, double* x, double* times);
+/* a solve with new right-hand sides against the factors of the last orc_solve */
+int orc_solve_again(void* h, int nrhs, const double* b, double* x);
 /* Multiply every matrix entry by (1 + rel*u), u a fixed pseudo-random number in
  * [-1, 1] per (i, j): used to measure how strongly the algorithm amplifies
  * last-bit differences in the entries. */

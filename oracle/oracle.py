@@ -56,6 +56,7 @@ def lib():
         _lib.orc_dense_matvec.argtypes = [v, ctypes.c_int, d, d]
         _lib.orc_total_field.argtypes = [v, ctypes.c_int, d, d, d]
         _lib.orc_solve.argtypes = [v, ctypes.c_int, d, d, d]
+        _lib.orc_solve_again.argtypes = [v, ctypes.c_int, d, d]
         _lib.orc_set_variant.argtypes = [v, ctypes.c_int]
         _lib.orc_set_schedule.argtypes = [v, ctypes.c_int]
         _lib.orc_compressions.argtypes = [v]
@@ -208,6 +209,14 @@ class Problem:
         t = np.zeros(4)
         lib().orc_solve(self.h, b.shape[0], _dp(bi), _dp(x), _dp(t))
         return x[..., 0] + 1j * x[..., 1], t
+
+    def solve_again(self, b):
+        """b: (nrhs, N) complex, against the factors of the last solve()."""
+        b = np.atleast_2d(b)
+        bi = np.ascontiguousarray(np.stack([b.real, b.imag], -1))
+        x = np.zeros_like(bi)
+        lib().orc_solve_again(self.h, b.shape[0], _dp(bi), _dp(x))
+        return x[..., 0] + 1j * x[..., 1]
 
     def level_ranks(self, level):
         n = 4 ** level

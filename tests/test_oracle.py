@@ -213,3 +213,24 @@ def test_oracle_elimination_solves_compressed_matrix(oracle_mod, table_cache, q_
     A = P.dense()
     xd = np.linalg.solve(A, b[0])
     assert np.linalg.norm(x_eff[0] - xd) / np.linalg.norm(xd) < 1e-3
+
+
+@pytest.mark.parametrize("q_kind,kappa,tol_pow", [("gaussian160", 10.0, 8), ("gauss_aw", 20.0, 10), ("disk", 20.0, 8)])
+def test_split_solve_algebra(oracle_mod, table_cache, q_kind, kappa, tol_pow):
+    """Solving new right-hand sides against kept factors: the elimination's
+    right-hand-side updates (F:1968, 1997-2001, 2252, 2289-2293) gathered per
+    receiving box, with the L2P_f fill-ins kept per neighbour slot, give the
+    same solution as carrying the new right-hand sides through the elimination
+    (to rounding: the products are summed in another order)."""
+    p, (M, near, _) = table_cache(depth=3, q_kind=q_kind, kappa=kappa, tol_pow=tol_pow)
+    P = oracle_mod.Problem(p, M, near)
+    b1 = P.rhs_plane_wave([0.4])
+    P.solve(b1)
+    b2 = P.rhs_plane_wave([1.3, 2.8])
+    x_again = P.solve_again(b2)
+    x_fresh, _ = oracle_mod.Problem(p, M, near).solve(b2)
+    rel = np.linalg.norm(x_again - x_fresh) / np.linalg.norm(x_fresh)
+    print("%s: split solve vs carried right-hand side %.2e" % (q_kind, rel))
+    # the smooth Gaussian's skeleton blocks are ill-conditioned: there the oracle's
+    # own solution moves by ~1e-7 under 1e-16 perturbations of the entries
+    assert rel <= (1e-7 if q_kind == "gauss_aw" else 1e-9)
