@@ -57,3 +57,13 @@ def test_invalid_description_is_rejected():
     h = ctypes.c_void_p()
     st = lib.aifmm_problem_create(ctypes.byref(d), 0, ctypes.byref(h))
     assert st != 0
+
+
+def test_server_refuses_to_start_without_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import aifmm_ls_b200 as A
+    with pytest.raises(A.AifmmError) as e:
+        A.Server(workers=1)
+    assert e.value.status == 6  # AIFMM_ERR_NODEVICE
