@@ -93,6 +93,7 @@ struct aifmm_server {
   std::map<long, std::unique_ptr<Req>> reqs;
   std::vector<std::thread> workers;
   bool stopping = false;
+  int factoring = 0;  // workers running a factorisation
   long next_id = 1;
   uint64_t tick = 0;
   // statistics
@@ -178,8 +179,11 @@ struct aifmm_server {
       bool have_solve = false;
       // factorisations that fit now come first: they unblock queued solves.  One
       // that does not fit yet stays queued while solves on resident keys run
-      // (their completion is what makes idle factors evictable).
-      for (auto it = factor_q.begin(); it != factor_q.end();) {
+      // (their completion is what makes idle factors evictable).  With more than
+      // one worker, one is always left for solves, which take milliseconds where
+      // a factorisation takes seconds.
+      const bool may_factor = (int)workers.size() < 2 || factoring < (int)workers.size() - 1;
+      for (auto it = factor_q.begin(); may_factor && it != factor_q.end();) {
         Req* r = *it;
         Factor& f = factors[r->key];
         if (f.busy) { ++it; continue; }
@@ -227,11 +231,13 @@ struct aifmm_server {
         const size_t need = estimate(f.desc);
         f.busy = true;
         f.reserve = need;
+        ++factoring;
         lk.unlock();
         std::string err;
         size_t bytes = 0;
         const aifmm_status st = build(f, err, bytes);
         lk.lock();
+        --factoring;
         f.busy = false;
         f.reserve = 0;
         f.queued_factor = false;
@@ -271,14 +277,23 @@ struct aifmm_server {
       lk.unlock();
       int N = 0;
       aifmm_num_points(p, &N);
-      std::vector<double> B((size_t)2 * N * tot), X((size_t)2 * N * tot);
+      // the batch is padded with zero columns to a power of two, so that each key
+      // needs at most log2(max_batch_rhs) + 1 solve graphs; padding changes no
+      // other column (every column is computed on its own)
+      int width = 1;
+      while (width < tot) width <<= 1;
+      if (width > max_batch_rhs) width = tot;
+      std::vector<double> B((size_t)2 * N * width, 0.0), X((size_t)2 * N * width);
       size_t o = 0;
       for (Req* r : batch) {
         std::memcpy(B.data() + o, r->b, sizeof(double) * 2 * (size_t)N * r->nrhs);
         o += (size_t)2 * N * r->nrhs;
       }
-      const aifmm_status st = aifmm_solve(p, tot, B.data(), N, X.data(), N, nullptr, AIFMM_PTR_HOST);
+      const aifmm_status st =
+          aifmm_solve(p, width, B.data(), N, X.data(), N, nullptr, AIFMM_PTR_HOST | AIFMM_SOLVE_GRAPH);
       std::string err = st == AIFMM_OK ? "" : aifmm_last_error(p);
+      double v[15] = {0};
+      aifmm_stats(p, v, 15);  // the graphs' buffers count towards the key's footprint
       o = 0;
       if (st == AIFMM_OK)
         for (Req* r : batch) {
@@ -287,6 +302,7 @@ struct aifmm_server {
         }
       lk.lock();
       f.busy = false;
+      f.bytes = (size_t)(v[13] + v[14]);
       f.last_use = ++tick;
       ++batches;
       batch_rhs_total += tot;

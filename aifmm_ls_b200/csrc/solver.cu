@@ -2418,7 +2418,7 @@ struct aifmm_problem {
   double tune_ms[2][2] = {{0, 0}, {0, 0}};  // [thin, wide][16, 32]
   void autotune() {
     const int r = rank, R = std::min(4 * rank, 160);
-    const int nb = std::max(256, std::min(4096, nBoxes[depth] / 2));
+    const int nb = std::max(256, std::min(4096, nleaf / 2));  // the tree need not be built yet
     struct Shape { int m, n, k; };
     const Shape thin[2] = {{r, 8, r}, {R, 8, R}}, wide[2] = {{r, r, r}, {R, R, R}};
     size_t elems = 0;
@@ -2685,8 +2685,9 @@ struct aifmm_problem {
       int e = aifmm_launch_colaxpby(xx, N, yy, N, N, nr, dab, dab + nr, st);
       if (e) throw Fail(AIFMM_ERR_CUDA, cudaGetErrorString((cudaError_t)e));
     };
-    auto precond = [&](const double2* in, double2* out) {  // out = M^-1 in
-      solve_rhs(nr, reinterpret_cast<const double*>(in), N, reinterpret_cast<double*>(out), N, AIFMM_PTR_DEVICE);
+    auto precond = [&](const double2* in, double2* out) {  // out = M^-1 in, one graph per nrhs
+      solve_rhs(nr, reinterpret_cast<const double*>(in), N, reinterpret_cast<double*>(out), N,
+                AIFMM_PTR_DEVICE | AIFMM_SOLVE_GRAPH);
     };
     const std::vector<double2> one(nr, C1), mone(nr, CM1), zero_(nr, C0);
     std::vector<double2> d;

@@ -260,7 +260,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the solve-latency measurement with kept factors")
     ap.add_argument("--no-peak", action="store_true", help="skip the cuBLAS FP64 peak measurement (profiling runs)")
     ap.add_argument("--batched", type=int, default=1, help="1: also run the 64-problem batched configuration")
-    ap.add_argument("--trace", type=float, default=60.0, help="seconds of the serving trace (0: skip)")
+    ap.add_argument("--trace", type=float, default=30.0, help="seconds of the serving trace (0: skip)")
     ap.add_argument("--no-kernel-profile", action="store_true",
                     help="skip the extra event-instrumented step that feeds the roofline (profiling runs)")
     args = ap.parse_args()
@@ -361,18 +361,6 @@ def main():
         t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3, pg, device)
     x = (x_pin if t_e2e is not None else x_dev.cpu()).numpy().view(np.complex128).reshape(NRHS, N)
     finite = bool(np.isfinite(x).all())
-    serving = None if args.no_serving else solve_latency(T, K, lib, stream, device, args)
-    extra = {}
-    if args.batched and rank == 0:
-        try:
-            extra["batched_uneven"] = batched_uneven(device)
-        except Exception as e:  # reported, never fatal for the headline measurement
-            extra["batched_uneven"] = {"error": repr(e)}
-    if args.trace > 0 and rank == 0:
-        try:
-            extra["serving_trace"] = serving_trace(device, seconds=args.trace)
-        except Exception as e:
-            extra["serving_trace"] = {"error": repr(e)}
     # one more step, untimed, with CUDA events around every launch of the dense
     # kernels: per-kernel durations and algorithmic flops for the roofline
     kinds = {0: "qr_factor", 1: "qr_solve", 2: "gemm"}
@@ -385,6 +373,24 @@ def main():
         prof = {kinds[kd]: T.kernel_profile_read(kd) for kd in kinds}
         for kd in kinds:
             T.kernel_profile(kd, False)
+    extra = {}
+    try:
+        serving = None if args.no_serving else solve_latency(T, K, lib, stream, device, args)
+    except Exception as e:  # reported, never fatal for the headline measurement
+        serving = {"error": repr(e)}
+    # the headline problem's assembly workspaces are not needed by what follows
+    lib.aifmm_trim(K.h)
+    torch.cuda.empty_cache()
+    if args.batched and rank == 0:
+        try:
+            extra["batched_uneven"] = batched_uneven(device)
+        except Exception as e:
+            extra["batched_uneven"] = {"error": repr(e)}
+    if args.trace > 0 and rank == 0:
+        try:
+            extra["serving_trace"] = serving_trace(device, seconds=args.trace)
+        except Exception as e:
+            extra["serving_trace"] = {"error": repr(e)}
     if rank == 0:
         peaks = measured_peaks()
         line = {
@@ -420,8 +426,9 @@ def main():
 def solve_latency(T, K, lib, stream, device, args, nrhs_list=(1, 8, 64)):
     """Latency of aifmm_solve against factors kept on the device (one factorisation,
     then W untimed and K timed solves per right-hand-side count; right-hand sides
-    and solutions resident in HBM).  Each solve is bracketed by CUDA events on the
-    solver's stream."""
+    and solutions resident in HBM), issued launch by launch ("eager") and replayed
+    as one CUDA graph ("graph"; its first call records the graph).  Each solve is
+    bracketed by CUDA events on the solver's stream."""
     import ctypes
     import torch
     T.createTree()
@@ -437,25 +444,33 @@ def solve_latency(T, K, lib, stream, device, args, nrhs_list=(1, 8, 64)):
         th = rng.uniform(0, 2 * np.pi, nr)
         b = torch.from_numpy(K.rhs_plane_wave(th).view(np.float64).copy()).to(f"cuda:{device}")
         x = torch.empty_like(b)
-        ms = []
-        launches = 0
-        for it in range(args.warmup + args.steps):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            st = lib.aifmm_solve(K.h, nr, ctypes.cast(b.data_ptr(), dp), N, ctypes.cast(x.data_ptr(), dp), N, None, 1)
-            e1.record(stream)
-            if st != 0:
-                raise RuntimeError(lib.aifmm_last_error(K.h).decode())
-            e1.synchronize()
-            if it >= args.warmup:
-                ms.append(e0.elapsed_time(e1))
-                launches = T.launch_counts_split()[1]
-        ms = np.array(ms)
-        out["nrhs_%d" % nr] = {"p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
-                               "mean_ms": float(ms.mean()), "solves": int(ms.size),
-                               "rhs_unknowns_per_s": float(N * nr / (ms.mean() * 1e-3)),
-                               "gpu_launches_per_solve": int(launches)}
+        res = {}
+        for mode, flags in (("eager", 1), ("graph", 1 | 4)):  # AIFMM_PTR_DEVICE, | AIFMM_SOLVE_GRAPH
+            ms = []
+            launches = 0
+            t_first = None
+            for it in range(args.warmup + args.steps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                h0 = time.perf_counter()
+                e0.record(stream)
+                st = lib.aifmm_solve(K.h, nr, ctypes.cast(b.data_ptr(), dp), N, ctypes.cast(x.data_ptr(), dp), N,
+                                     None, flags)
+                e1.record(stream)
+                if st != 0:
+                    raise RuntimeError(lib.aifmm_last_error(K.h).decode())
+                e1.synchronize()
+                if it == 0:
+                    t_first = 1e3 * (time.perf_counter() - h0)
+                if it >= args.warmup:
+                    ms.append(e0.elapsed_time(e1))
+                    launches = T.launch_counts_split()[1]
+            ms = np.array(ms)
+            res[mode] = {"p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
+                         "mean_ms": float(ms.mean()), "solves": int(ms.size), "first_call_ms": t_first,
+                         "rhs_unknowns_per_s": float(N * nr / (ms.mean() * 1e-3)),
+                         "gpu_launches_per_solve": int(launches)}
+        out["nrhs_%d" % nr] = res
         del b, x
     return out
 
@@ -505,23 +520,60 @@ def batched_uneven(device, nprob=64, workers=4, seed=SEED + 3):
             "server": stats}
 
 
-def serving_trace(device, seconds=60.0, rate=200.0, workers=4, seed=SEED + 4):
+class _PlaneWaves:
+    """Plane-wave right-hand sides b = -kappa^2 q(x) exp(i kappa (x cos t + y sin t))
+    (LS/LS_functions.hpp:113-120) computed on the host from one grid per depth, so
+    that the trace needs no solver handle per geometry.  The first geometry of each
+    depth is checked against the library's own aifmm_rhs_plane_wave."""
+
+    def __init__(self, A):
+        self.A = A
+        self.grids = {}
+
+    @staticmethod
+    def contrast(kw, xy):
+        R2 = (xy ** 2).sum(1)
+        if kw["q_kind"] == "gauss_aw":
+            return kw["q_amp"] * np.exp(-kw["q_width"] * R2)
+        return np.where(R2 < kw["q_radius"] ** 2, kw["q_amp"], 0.0)
+
+    def __call__(self, kw, thetas):
+        d = kw["depth"]
+        th = np.atleast_1d(thetas)
+        if d not in self.grids:
+            K = self.A.LSKernel(**kw)
+            self.grids[d] = K.gridPoints
+            want = K.rhs_plane_wave(th)
+            K.close()
+            got = self._b(kw, self.grids[d], th)
+            if not np.allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max()):
+                raise RuntimeError("host plane waves disagree with aifmm_rhs_plane_wave")
+        return self._b(kw, self.grids[d], th)
+
+    def _b(self, kw, xy, th):
+        q = self.contrast(kw, xy)
+        ph = kw["kappa"] * (np.outer(np.cos(th), xy[:, 0]) + np.outer(np.sin(th), xy[:, 1]))
+        return -kw["kappa"] ** 2 * q[None, :] * np.exp(1j * ph)
+
+
+def serving_trace(device, seconds=30.0, rate=200.0, workers=4, seed=SEED + 4):
     """Poisson arrivals at `rate` req/s for `seconds`: 5% factorize requests for new
-    geometries (depth U{5,6}, problem as the batched configuration), 95% solve requests
-    of U{1..64} plane waves against a random resident geometry.  Latency = submission to
-    completion (host clock); the engine batches the solves queued for a geometry."""
+    geometries (depth 5, problem as the batched configuration), 95% solve requests
+    of U{1..64} plane waves against a random geometry already submitted.  Latency =
+    submission to completion (host clock); the engine batches the solves queued for
+    a geometry."""
     import aifmm_ls_b200 as A
     rng = np.random.default_rng(seed)
+    waves = _PlaneWaves(A)
     S = A.Server(device=device, workers=workers, max_batch_rhs=64)
     lat = {"solve": [], "factorize": []}
     try:
         keys = []
         # a few geometries resident before the clock starts
         for key in range(4):
-            kw = _random_problem(rng, rng.integers(5, 7))
+            kw = _random_problem(rng, 5)
             S.wait(S.factorize(key, **kw), timeout=3600)
             keys.append((key, kw))
-        Ks = {}
         pending = []
         t0 = time.perf_counter()
         t_next = t0
@@ -538,15 +590,13 @@ def serving_trace(device, seconds=60.0, rate=200.0, workers=4, seed=SEED + 4):
             nreq += 1
             if rng.uniform() < 0.05:
                 key = len(keys)
-                kw = _random_problem(rng, rng.integers(5, 7))
+                kw = _random_problem(rng, 5)
                 keys.append((key, kw))
                 pending.append(("factorize", S.factorize(key, **kw), 0))
             else:
-                key, kw = keys[int(rng.integers(0, min(len(keys), 4 + len(keys) // 2)))]
-                if key not in Ks:
-                    Ks[key] = A.LSKernel(**kw)
+                key, kw = keys[int(rng.integers(0, len(keys)))]
                 nr = int(rng.integers(1, 65))
-                b = Ks[key].rhs_plane_wave(rng.uniform(0, 2 * np.pi, nr))
+                b = waves(kw, rng.uniform(0, 2 * np.pi, nr))
                 pending.append(("solve", S.solve(key, b), b.size))
         failed = 0
         for kind, rid, nunk in pending:
@@ -562,8 +612,9 @@ def serving_trace(device, seconds=60.0, rate=200.0, workers=4, seed=SEED + 4):
         S.close()
     out = {"seconds": seconds, "rate_req_per_s": rate, "requests": nreq, "failed": failed, "wall_s": wall,
            "rhs_unknowns_per_s": solved_unknowns / wall, "server": stats,
-           "note": "trace shortened from 10 minutes; factorize depths 5-6 (a depth-7 factorisation takes "
-                   "seconds, far longer than the mean gap between factorize requests at 5% of 200 req/s)"}
+           "note": "trace shortened from 10 minutes to keep the benchmark within minutes; new geometries at "
+                   "depth 5 (a depth-7 factorisation takes seconds, longer than the mean gap between factorize "
+                   "requests at 5% of 200 req/s); wall_s includes draining the queue after the last arrival"}
     for kind, v in lat.items():
         if v:
             out[kind] = {"count": len(v), "p50_ms": float(np.percentile(v, 50)), "p99_ms": float(np.percentile(v, 99))}

@@ -37,6 +37,22 @@ def test_grid_and_rhs_match_oracle(oracle_mod, table_cache):
     assert np.max(np.abs(b - bo)) <= 1e-13 * np.max(np.abs(bo))
 
 
+def _round6_kat(gpu, ora):
+    """Survey KAT 6: the tables after the reference's 6-digit text round trip.
+    About a fifth of the real and imaginary parts vanish by symmetry; both
+    implementations leave rounding noise there (< 1e-12 of the table's scale),
+    which the text round trip keeps and which no two implementations share.
+    Every significant part must be bit-identical; noise parts must agree to
+    1e-12 of the scale.  Returns (flips among significant parts, parts)."""
+    a = np.concatenate([gpu.real.ravel(), gpu.imag.ravel()])
+    b = np.concatenate([ora.real.ravel(), ora.imag.ravel()])
+    scale = np.max(np.abs(b))
+    sig = np.abs(b) >= 1e-12 * scale
+    flips = int(np.count_nonzero(a[sig] != b[sig]))
+    assert np.max(np.abs(a[~sig] - b[~sig])) <= 1e-12 * scale
+    return flips, int(sig.sum())
+
+
 def test_gpu_tables_match_oracle(oracle_mod):
     import aifmm_ls_b200 as A
     p = oracle_mod.params(depth=3, kappa=10.0)
@@ -44,22 +60,15 @@ def test_gpu_tables_match_oracle(oracle_mod):
     K = A.LSKernel(depth=3, kappa=10.0)
     K.tables_compute(round6=False)
     M1, N1 = K.tables_get()
-    # same adaptive quadrature (absolute tolerance 1e-7 per integral)
-    assert np.max(np.abs(M1 - M0)) <= 1e-6 * max(1.0, np.max(np.abs(M0)))
-    assert np.max(np.abs(N1 - N0)) <= 1e-6 * max(1.0, np.max(np.abs(N0)))
-    # after the 6-digit round trip the two sides differ by at most the quadrature
-    # tolerance plus one unit in the sixth digit; most values are bit-identical
+    # same adaptive quadrature (absolute tolerance 1e-7 per integral): the values agree far below it
+    for a, b in ((M1, M0), (N1, N0)):
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(b))
     M0r, N0r, _ = oracle_mod.tables(p, round6=True)
     K.tables_compute(round6=True)
     M1r, N1r = K.tables_get()
-    for a, b in ((M1r, M0r), (N1r, N0r)):
-        scale = np.max(np.abs(b))
-        assert np.max(np.abs(a - b)) <= 2e-6 * scale
-    vals0 = np.concatenate([M0r.ravel(), N0r.ravel()])
-    vals1 = np.concatenate([M1r.ravel(), N1r.ravel()])
-    flips = np.count_nonzero(vals0 != vals1)
-    print("6-digit table values differing between GPU and oracle: %d of %d" % (flips, vals0.size))
-    assert flips <= 0.10 * vals0.size, flips
+    flips, nsig = _round6_kat(np.concatenate([M1r.ravel(), N1r.ravel()]), np.concatenate([M0r.ravel(), N0r.ravel()]))
+    print("6-digit tables: significant parts differing between GPU and oracle: %d of %d" % (flips, nsig))
+    assert flips == 0
 
 
 @pytest.mark.parametrize("q_kind,kappa", [("gaussian160", 10.0), ("gauss_aw", 40.0), ("disk", 80.0)])
@@ -204,7 +213,12 @@ def test_reference_default_run_depth5(oracle_mod, table_cache):
     """The reference's default run `testFMM2D_find_error 6 10 6 1 0 8 5`
     (testFMM2D_find_error.cpp:44-52, Readme.md:17-21): 6x6 nodes, kappa 10,
     degree 6, Qchoice 0, TOL 1e-8, depth 5 (36,864 unknowns), one plane wave at
-    theta = 0.  The GPU solution matches the oracle's to the flat 1e-8."""
+    theta = 0.  At this depth the reference algorithm itself resolves x only to
+    ~1e-5: perturbing every entry by 1e-16 moves the oracle's solution by
+    3e-6 .. 4e-4 (rank and pivot decisions near their thresholds).  So the bound
+    is the one of test_solution_matches_oracle, max(1e-8, 5 x that spread), and
+    the GPU solution must be as accurate as the oracle's: its residual with
+    exact entries on 400 sampled rows within 10% of the oracle solution's."""
     import aifmm_ls_b200 as A
     p, tabs = table_cache(depth=5, q_kind="gaussian160", kappa=10.0, tol_pow=8)
     M, near = tabs[:2]
@@ -217,8 +231,21 @@ def test_reference_default_run_depth5(oracle_mod, table_cache):
     xo, _ = P.solve(b)
     x = T.solve(b)
     rel = np.linalg.norm(x - xo) / np.linalg.norm(xo)
-    print("depth 5 reference run: |x_gpu - x_oracle| / |x_oracle| = %.2e" % rel)
-    assert rel <= SOLVE_TOL
+    spread = 0.0
+    for eps in (1e-16, -1e-16):
+        Q = oracle_mod.Problem(p, M, near)
+        Q.set_perturbation(eps)
+        x1, _ = Q.solve(b)
+        spread = max(spread, np.linalg.norm(x1 - xo) / np.linalg.norm(xo))
+    rng = np.random.default_rng(5)
+    rows = np.sort(rng.choice(K.N, 400, replace=False)).astype(np.int32)
+    Ar = K.getMatrix(rows, np.arange(K.N, dtype=np.int32))
+    res_g = np.linalg.norm(Ar @ x[0] - b[0, rows]) / np.linalg.norm(b[0, rows])
+    res_o = np.linalg.norm(Ar @ xo[0] - b[0, rows]) / np.linalg.norm(b[0, rows])
+    print("depth 5 reference run: |x_gpu - x_oracle| = %.2e, oracle spread %.2e; sampled residual GPU %.3e, "
+          "oracle %.3e" % (rel, spread, res_g, res_o))
+    assert rel <= max(SOLVE_TOL, 5.0 * spread)
+    assert res_g <= 1.1 * res_o + 1e-12
 
 
 def test_bench_path_with_gpu_tables(oracle_mod):
@@ -237,13 +264,10 @@ def test_bench_path_with_gpu_tables(oracle_mod):
     M1r, N1r = K.tables_get()
     v0 = np.concatenate([M0.ravel(), N0.ravel()])
     v1 = np.concatenate([M1.ravel(), N1.ravel()])
-    w0 = np.concatenate([M0r.ravel(), N0r.ravel()])
-    w1 = np.concatenate([M1r.ravel(), N1r.ravel()])
-    ok = np.abs(v0) > 0
-    rel_unrounded = np.max(np.abs(v1 - v0)[ok] / np.abs(v0)[ok])
-    flips = int(np.count_nonzero(w0 != w1))
-    print("tables before rounding: max relative difference %.2e; 6-digit values differing: %d of %d"
-          % (rel_unrounded, flips, w0.size))
+    rel_unrounded = np.max(np.abs(v1 - v0)) / np.max(np.abs(v0))
+    flips, nsig = _round6_kat(np.concatenate([M1r.ravel(), N1r.ravel()]), np.concatenate([M0r.ravel(), N0r.ravel()]))
+    print("tables before rounding: max difference %.2e of the scale; 6-digit significant parts differing: %d of %d"
+          % (rel_unrounded, flips, nsig))
     T = A.FMM2DTree(K)
     T.createTree()
     T.assemble()
@@ -255,5 +279,6 @@ def test_bench_path_with_gpu_tables(oracle_mod):
     rel = np.linalg.norm(x - xo) / np.linalg.norm(xo)
     spread = _oracle_spread(oracle_mod, p, M0r, N0r, b, xo)
     print("bench path: |x_gpu(gpu tables) - x_oracle(oracle tables)| = %.2e, oracle spread %.2e" % (rel, spread))
-    assert rel_unrounded <= 1e-9
-    assert rel <= max(SOLVE_TOL, 5.0 * spread, 1e-6), (rel, spread)
+    assert rel_unrounded <= 1e-12
+    assert flips == 0
+    assert rel <= max(SOLVE_TOL, 5.0 * spread), (rel, spread)
