@@ -78,6 +78,7 @@ SIGNATURES = {
                              _i, _d, ctypes.c_int], ctypes.c_int),
     "aifmm_server_create": ([ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _P(_v)], ctypes.c_int),
     "aifmm_server_destroy": ([_v], ctypes.c_int),
+    "aifmm_server_set_factor_workers": ([_v, ctypes.c_int], ctypes.c_int),
     "aifmm_server_factorize": ([_v, ctypes.c_longlong, _P(Desc), _P(ctypes.c_long)], ctypes.c_int),
     "aifmm_server_solve": ([_v, ctypes.c_longlong, ctypes.c_int, _d, _d, _P(ctypes.c_long)], ctypes.c_int),
     "aifmm_server_wait": ([_v, ctypes.c_long, ctypes.c_double, _i, _d, _i], ctypes.c_int),
@@ -414,13 +415,15 @@ class Server:
     STAT_KEYS = ["solve_p50_ms", "solve_p99_ms", "factorize_p50_ms", "factorize_p99_ms", "solves", "factorizations",
                  "evictions", "batches", "mean_batch_rhs", "bytes_in_use", "resident", "failed"]
 
-    def __init__(self, device=0, hbm_budget_bytes=0.0, workers=2, max_batch_rhs=64):
+    def __init__(self, device=0, hbm_budget_bytes=0.0, workers=2, max_batch_rhs=64, factor_workers=None):
         h = _v()
         st = load().aifmm_server_create(device, float(hbm_budget_bytes), workers, max_batch_rhs, ctypes.byref(h))
         if st != 0:
             raise AifmmError(st, load().aifmm_status_string(st).decode())
         self.h = h
         self._bufs = {}
+        if factor_workers is not None:
+            load().aifmm_server_set_factor_workers(self.h, int(factor_workers))
 
     def close(self):
         if getattr(self, "h", None):

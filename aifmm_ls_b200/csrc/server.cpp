@@ -93,7 +93,8 @@ struct aifmm_server {
   std::map<long, std::unique_ptr<Req>> reqs;
   std::vector<std::thread> workers;
   bool stopping = false;
-  int factoring = 0;  // workers running a factorisation
+  int factoring = 0;    // workers running a factorisation
+  int factor_cap = -1;  // at most this many at once (< 0: all workers but one)
   long next_id = 1;
   uint64_t tick = 0;
   // statistics
@@ -180,9 +181,11 @@ struct aifmm_server {
       // factorisations that fit now come first: they unblock queued solves.  One
       // that does not fit yet stays queued while solves on resident keys run
       // (their completion is what makes idle factors evictable).  With more than
-      // one worker, one is always left for solves, which take milliseconds where
-      // a factorisation takes seconds.
-      const bool may_factor = (int)workers.size() < 2 || factoring < (int)workers.size() - 1;
+      // one worker, by default one is always left for solves, which take
+      // milliseconds where a factorisation takes seconds
+      // (aifmm_server_set_factor_workers changes the share).
+      const int cap = factor_cap > 0 ? factor_cap : std::max(1, (int)workers.size() - 1);
+      const bool may_factor = factoring < cap;
       for (auto it = factor_q.begin(); may_factor && it != factor_q.end();) {
         Req* r = *it;
         Factor& f = factors[r->key];
@@ -348,6 +351,14 @@ aifmm_status aifmm_server_destroy(aifmm_server* s) {
   for (auto& kv : s->factors)
     if (kv.second.p) aifmm_problem_destroy(kv.second.p);
   delete s;
+  return AIFMM_OK;
+}
+
+aifmm_status aifmm_server_set_factor_workers(aifmm_server* s, int n) {
+  if (!s || n < 1) return AIFMM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->factor_cap = std::min(n, (int)s->workers.size());
+  s->cv_work.notify_all();
   return AIFMM_OK;
 }
 

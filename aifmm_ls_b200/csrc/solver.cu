@@ -96,10 +96,11 @@ class Pool {
       return p;
     }
     if (left_ < c) {
-      size_t sz = size_t(512) << 20;
+      const size_t sz = slab_;
       void* p = nullptr;
       CK(cudaMalloc(&p, sz));
       slabs_.push_back(p);
+      slab_bytes_ += sz;
       cur_ = static_cast<char*>(p);
       left_ = sz;
     }
@@ -117,10 +118,17 @@ class Pool {
     for (void* p : slabs_) cudaFree(p);
     for (auto& kv : big_) cudaFree(kv.first);
     slabs_.clear(); big_.clear(); free_.clear(); pending_.clear();
-    cur_ = nullptr; left_ = 0;
+    cur_ = nullptr; left_ = 0; slab_bytes_ = 0;
+  }
+  // slab size: a power of two from 64 MB (the largest block a slab serves) to 512 MB,
+  // so that a small problem does not hold half a gigabyte it never uses
+  void set_slab(size_t bytes) {
+    size_t s = size_t(64) << 20;
+    while (s < bytes && s < (size_t(512) << 20)) s <<= 1;
+    slab_ = s;
   }
   size_t reserved() const {
-    size_t b = slabs_.size() * (size_t(512) << 20);
+    size_t b = slab_bytes_;
     for (auto& kv : big_) b += kv.second;
     return b;
   }
@@ -128,6 +136,7 @@ class Pool {
  private:
   static size_t cls(size_t b) { size_t c = 256; while (c < b) c <<= 1; return c; }
   std::vector<void*> slabs_;
+  size_t slab_ = size_t(512) << 20, slab_bytes_ = 0;
   std::vector<std::pair<void*, size_t>> big_;
   std::map<size_t, std::vector<void*>> free_;
   std::vector<std::pair<void*, size_t>> pending_;
@@ -815,7 +824,8 @@ struct aifmm_problem {
     tol = std::pow(10, -1.0 * d.tol_pow);
     tol_factor = tol;
     stage.init(size_t(64) << 20, st, st2);
-    // per-step scratch: ~1 KB per unknown (2 GB at 589,824 unknowns), at least 64 MB
+    pool.set_slab((size_t)N * 2048);  // 512 MB slabs from ~260,000 unknowns up
+    // per-step scratch: ~3.6 KB per unknown (2 GB at 589,824 unknowns), at least 64 MB
     scratch.init(std::min(size_t(2) << 30, std::max(size_t(64) << 20, (size_t)N * 3600)));
     CK(cudaMalloc(&d_pts, sizeof(double2) * N));
     CK(cudaMalloc(&d_q, sizeof(double) * N));
@@ -2156,19 +2166,16 @@ struct aifmm_problem {
   // particles of its neighbours with a larger index (already solved) and the
   // multipoles of the others (known from the level above).  The backward waves
   // give each box exactly what the sequential order gives it.
+  // The particle right-hand side sr and the multipoles are updated in place: sr
+  // is read by this box alone, and a box's multipoles only by its larger-index
+  // neighbours, which earlier waves have finished (a parent's particles, which
+  // hold its children's multipoles, are not read again either).
   void backward_wave(int j, const std::vector<int>& ks) {
-    struct Work { Blk rhs1, t, rhs2, v; };
-    std::vector<Work> wk(ks.size());
+    std::vector<Blk> t(ks.size());
     std::vector<int> act;  // boxes with unknowns at this level
     for (size_t q = 0; q < ks.size(); ++q)
       if (T[j][ks[q]].P2P[ks[q]].size() != 0) act.push_back((int)q);
-    for (int q : act) {
-      Box& B = T[j][ks[q]];
-      wk[q].rhs1 = scr(B.P2P[ks[q]].r, nrhs);
-      copy(wk[q].rhs1, B.sr);
-    }
-    flush_geam();
-    for (int q : act) {
+    for (int q : act) {  // rhs1 = sr - sum of the neighbours' products
       const int k = ks[q];
       Box& B = T[j][k];
       std::vector<std::pair<Blk, Blk>> terms;
@@ -2178,41 +2185,30 @@ struct aifmm_problem {
         if (nn > k) terms.push_back({B.P2P[nn], T[j][nn].particles});
         else terms.push_back({B.M2P[nn], T[j][nn].multipoles});
       }
-      gemm_sum(wk[q].rhs1, terms, CM1, C1);
+      gemm_sum(B.sr, terms, CM1, C1);
     }
     flush_gemm();
-    for (int q : act) {
+    for (int q : act) {  // t = QRx^-1 rhs1
       Box& B = T[j][ks[q]];
-      wk[q].t = scr(B.P2P[ks[q]].c, nrhs);
-      solve(B.qx, wk[q].rhs1, wk[q].t, C1);
+      t[q] = scr(B.P2P[ks[q]].c, nrhs);
+      solve(B.qx, B.sr, t[q], C1);
     }
     flush_solve();
-    for (int q : act) {
-      Box& B = T[j][ks[q]];
-      wk[q].rhs2 = scr(B.P2M.r, nrhs);
-      copy(wk[q].rhs2, B.multipoles);
-    }
-    flush_geam();
-    for (int q : act) gemm(wk[q].rhs2, T[j][ks[q]].P2M, 0, wk[q].t, 0, CM1, C1);
+    for (int q : act) gemm(T[j][ks[q]].multipoles, T[j][ks[q]].P2M, 0, t[q], 0, CM1, C1);  // rhs2
     flush_gemm();
-    for (int q : act) {
+    for (int q : act) {  // locals = QRz^-1 rhs2
       Box& B = T[j][ks[q]];
       Blk loc = newblk(B.L2M_f.size() != 0 ? B.L2M_f.c : 0, nrhs);
-      if (B.L2M_f.size() != 0) solve(B.qz, wk[q].rhs2, loc, C1);
+      if (B.L2M_f.size() != 0) solve(B.qz, B.multipoles, loc, C1);
       assign(B.locals, loc);
     }
     flush_solve();
-    for (int q : act) {
-      wk[q].v = scr(wk[q].rhs1.r, nrhs);
-      copy(wk[q].v, wk[q].rhs1);
-    }
-    flush_geam();
-    for (int q : act) gemm(wk[q].v, T[j][ks[q]].L2P, 0, T[j][ks[q]].locals, 0, CM1, C1);
+    for (int q : act) gemm(T[j][ks[q]].sr, T[j][ks[q]].L2P, 0, T[j][ks[q]].locals, 0, CM1, C1);  // v = rhs1 - L2P locals
     flush_gemm();
-    for (int q : act) {
+    for (int q : act) {  // particles = QRx^-1 v
       Box& B = T[j][ks[q]];
       Blk px = newblk(B.P2P[ks[q]].c, nrhs);
-      solve(B.qx, wk[q].v, px, C1);
+      solve(B.qx, B.sr, px, C1);
       assign(B.particles, px);
     }
     flush_solve();

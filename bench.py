@@ -260,6 +260,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the solve-latency measurement with kept factors")
     ap.add_argument("--no-peak", action="store_true", help="skip the cuBLAS FP64 peak measurement (profiling runs)")
     ap.add_argument("--batched", type=int, default=1, help="1: also run the 64-problem batched configuration")
+    ap.add_argument("--refined", type=int, default=1, help="1: also time the refined form (GMRES) on the same problem")
     ap.add_argument("--trace", type=float, default=30.0, help="seconds of the serving trace (0: skip)")
     ap.add_argument("--no-kernel-profile", action="store_true",
                     help="skip the extra event-instrumented step that feeds the roofline (profiling runs)")
@@ -378,9 +379,19 @@ def main():
         serving = None if args.no_serving else solve_latency(T, K, lib, stream, device, args)
     except Exception as e:  # reported, never fatal for the headline measurement
         serving = {"error": repr(e)}
+    if args.refined and rank == 0:
+        try:
+            extra["refined_vs_plain"] = refined_vs_plain(T, K, th, value, x)
+        except Exception as e:
+            extra["refined_vs_plain"] = {"error": repr(e)}
     # the headline problem's assembly workspaces are not needed by what follows
     lib.aifmm_trim(K.h)
     torch.cuda.empty_cache()
+    if args.refined and rank == 0:
+        try:
+            extra["refined_c3_physics"] = refined_c3(device)
+        except Exception as e:
+            extra["refined_c3_physics"] = {"error": repr(e)}
     if args.batched and rank == 0:
         try:
             extra["batched_uneven"] = batched_uneven(device)
@@ -475,6 +486,68 @@ def solve_latency(T, K, lib, stream, device, args, nrhs_list=(1, 8, 64)):
     return out
 
 
+def _refined_run(T, K, b, factor_tol_pow, rtol):
+    """createTree + assemble + factorise (recompression tolerance 10^-factor_tol_pow,
+    assembly kept) + GMRES to rtol; host wall clock per phase."""
+    T.set_factor_tolerance(factor_tol_pow)
+    try:
+        t0 = time.perf_counter()
+        T.createTree()
+        T.assemble()
+        t1 = time.perf_counter()
+        T.factorize(keep_assembly=True)
+        t2 = time.perf_counter()
+        x, iters, relres = T.solve_refined(b, rtol=rtol, maxit=90)
+        t3 = time.perf_counter()
+    finally:
+        T.set_factor_tolerance(0)
+    return x, {"assemble_s": t1 - t0, "factorize_s": t2 - t1, "gmres_s": t3 - t2, "total_s": t3 - t0,
+               "gmres_iterations": iters, "relative_residual": relres}
+
+
+def refined_vs_plain(T, K, th, plain_value, x_plain):
+    """The refined form on the benchmark problem itself: the same assembly (ACA
+    tolerance 1e-10), the factorisation at recompression tolerance 1e-6, FP64 GMRES
+    against the compressed operator to relative residual 1e-10, for the same 8
+    right-hand sides; against the plain FP64 direct solve of the timed steps."""
+    b = K.rhs_plane_wave(th)
+    x, out = _refined_run(T, K, b, 6, 1e-10)
+    N = K.N
+    out["unknowns_per_s"] = N / out["total_s"]
+    out["plain_fp64_unknowns_per_s"] = plain_value
+    out["refined_over_plain"] = out["unknowns_per_s"] / plain_value
+    out["rel_diff_to_plain_solution"] = float(np.linalg.norm(x - x_plain) / np.linalg.norm(x_plain))
+    out["timing"] = "host wall clock of one run (tree, assembly, factorisation, GMRES with host buffers)"
+    return out
+
+
+def refined_c3(device, depth=6, nrhs=32, seed=SEED + 2):
+    """The mixed-precision configuration's physics (8x8 nodes, kappa 80, disk q = 2 for
+    |x| < 0.5, NCA tolerance 1e-6, 32 plane waves, refinement to 1e-10) at depth 6
+    (262,144 unknowns), in this build's refined form: FP64 factorisation at the
+    problem's tolerance as the preconditioner of FP64 GMRES against the compressed
+    operator."""
+    import aifmm_ls_b200 as A
+    K = A.LSKernel(n_cheb=8, kappa=80.0, degree=6, depth=depth, tol_pow=6, q_kind="disk", q_amp=2.0, q_radius=0.5,
+                   device=device)
+    try:
+        t0 = time.perf_counter()
+        K.tables_compute(round6=True)
+        t_tab = time.perf_counter() - t0
+        T = A.FMM2DTree(K)
+        rng = np.random.default_rng(seed)
+        b = K.rhs_plane_wave(rng.uniform(0, 2 * np.pi, nrhs))
+        x, out = _refined_run(T, K, b, 0, 1e-10)
+        xd = T.solve_factored(b)  # the direct solve alone, same factors
+        r_direct = float(np.max(np.linalg.norm(b - T.compressed_matvec(xd), axis=1) / np.linalg.norm(b, axis=1)))
+    finally:
+        K.close()
+    out.update({"depth": depth, "unknowns": K.N, "nrhs": nrhs, "tables_s": t_tab,
+                "unknowns_per_s": K.N / out["total_s"], "direct_solve_relative_residual": r_direct,
+                "note": "depth 6 instead of 7 (8x8 nodes); factorisation FP64 (no complex64 arithmetic is built)"})
+    return out
+
+
 def _random_problem(rng, depth):
     """A problem of the batched / serving configurations: 6x6 nodes, kappa log-uniform in
     [5, 60], contrast a Gaussian of amplitude U[0.5, 2] (width 32) or a disk of radius
@@ -495,7 +568,7 @@ def batched_uneven(device, nprob=64, workers=4, seed=SEED + 3):
     import aifmm_ls_b200 as A
     rng = np.random.default_rng(seed)
     probs = [_random_problem(rng, rng.integers(4, 8)) for _ in range(nprob)]
-    S = A.Server(device=device, workers=workers, max_batch_rhs=64)
+    S = A.Server(device=device, workers=workers, max_batch_rhs=64, factor_workers=workers)
     try:
         t0 = time.perf_counter()
         fids = [S.factorize(i, **kw) for i, kw in enumerate(probs)]
@@ -556,7 +629,7 @@ class _PlaneWaves:
         return -kw["kappa"] ** 2 * q[None, :] * np.exp(1j * ph)
 
 
-def serving_trace(device, seconds=30.0, rate=200.0, workers=4, seed=SEED + 4):
+def serving_trace(device, seconds=30.0, rate=200.0, workers=8, seed=SEED + 4):
     """Poisson arrivals at `rate` req/s for `seconds`: 5% factorize requests for new
     geometries (depth 5, problem as the batched configuration), 95% solve requests
     of U{1..64} plane waves against a random geometry already submitted.  Latency =
@@ -565,7 +638,7 @@ def serving_trace(device, seconds=30.0, rate=200.0, workers=4, seed=SEED + 4):
     import aifmm_ls_b200 as A
     rng = np.random.default_rng(seed)
     waves = _PlaneWaves(A)
-    S = A.Server(device=device, workers=workers, max_batch_rhs=64)
+    S = A.Server(device=device, workers=workers, max_batch_rhs=64, factor_workers=workers // 2)
     lat = {"solve": [], "factorize": []}
     try:
         keys = []

@@ -258,6 +258,9 @@ aifmm_status aifmm_server_create(int device, double hbm_budget_bytes, int worker
                                  aifmm_server** out);
 /* Runs the queued requests to completion, then stops the workers and frees every factor. */
 aifmm_status aifmm_server_destroy(aifmm_server* s);
+/* How many workers may run factorisations at once (default: all but one, so that
+ * solves are never all stuck behind factorisations; 1 worker: that one). */
+aifmm_status aifmm_server_set_factor_workers(aifmm_server* s, int n);
 /* Queue a factorisation of desc under key (tables with the 6-digit round trip, tree,
  * assembly, FP64 factorisation); replaces an earlier one under the same key. */
 aifmm_status aifmm_server_factorize(aifmm_server* s, long long key, const aifmm_desc* desc, long* request);
