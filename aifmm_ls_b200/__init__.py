@@ -25,6 +25,7 @@ _lib = None
 
 PTR_HOST, PTR_DEVICE, KEEP_ASSEMBLY, SOLVE_GRAPH = 0, 1, 2, 4
 PRECISION_FP64 = 0
+PRECISION_C64 = 1   # the mixed form: complex64 elimination, FP64 refinement (solve_refined)
 Q_KINDS = {"gaussian160": 0, "multi_gauss": 1, "plasma": 2, "flatbump": 3, "cavity": 4, "lens": 5,
            "gauss_aw": 10, "disk": 11}
 
@@ -79,6 +80,7 @@ SIGNATURES = {
     "aifmm_server_create": ([ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _P(_v)], ctypes.c_int),
     "aifmm_server_destroy": ([_v], ctypes.c_int),
     "aifmm_server_set_factor_workers": ([_v, ctypes.c_int], ctypes.c_int),
+    "aifmm_server_set_form": ([_v, ctypes.c_int, ctypes.c_double], ctypes.c_int),
     "aifmm_server_factorize": ([_v, ctypes.c_longlong, _P(Desc), _P(ctypes.c_long)], ctypes.c_int),
     "aifmm_server_solve": ([_v, ctypes.c_longlong, ctypes.c_int, _d, _d, _P(ctypes.c_long)], ctypes.c_int),
     "aifmm_server_wait": ([_v, ctypes.c_long, ctypes.c_double, _i, _d, _i], ctypes.c_int),
@@ -305,8 +307,10 @@ class FMM2DTree:
         return x
 
     # eliminate_phase_efficient + the base-level factorisation, right-hand side not carried (F:2407-2485)
-    def factorize(self, keep_assembly=False):
-        self._ck(load().aifmm_factorize(self.K.h, PRECISION_FP64, KEEP_ASSEMBLY if keep_assembly else 0))
+    def factorize(self, keep_assembly=False, precision=PRECISION_FP64):
+        """eliminate_phase_efficient without a right-hand side; precision PRECISION_C64 runs
+        the elimination and later solves in complex64 (refine with solve_refined)"""
+        self._ck(load().aifmm_factorize(self.K.h, precision, KEEP_ASSEMBLY if keep_assembly else 0))
 
     def set_factor_tolerance(self, tol_pow):
         """recompression tolerance 10^-tol_pow of the next factorisations (0: the problem's)"""
@@ -413,9 +417,13 @@ class Server:
     memory with LRU eviction.  Requests return ids; ``wait`` returns the result."""
 
     STAT_KEYS = ["solve_p50_ms", "solve_p99_ms", "factorize_p50_ms", "factorize_p99_ms", "solves", "factorizations",
-                 "evictions", "batches", "mean_batch_rhs", "bytes_in_use", "resident", "failed"]
+                 "evictions", "batches", "mean_batch_rhs", "bytes_in_use", "resident", "failed",
+                 "mean_gmres_iterations", "promoted_to_fp64"]
 
-    def __init__(self, device=0, hbm_budget_bytes=0.0, workers=2, max_batch_rhs=64, factor_workers=None):
+    def __init__(self, device=0, hbm_budget_bytes=0.0, workers=2, max_batch_rhs=64, factor_workers=None,
+                 precision=PRECISION_FP64, rtol=1e-8):
+        """precision PRECISION_C64: the mixed form (complex64 factors, every solve refined
+        by FP64 GMRES to relative residual rtol)"""
         h = _v()
         st = load().aifmm_server_create(device, float(hbm_budget_bytes), workers, max_batch_rhs, ctypes.byref(h))
         if st != 0:
@@ -424,6 +432,11 @@ class Server:
         self._bufs = {}
         if factor_workers is not None:
             load().aifmm_server_set_factor_workers(self.h, int(factor_workers))
+        if precision != PRECISION_FP64:
+            st = load().aifmm_server_set_form(self.h, int(precision), float(rtol))
+            if st != 0:
+                self.close()
+                raise AifmmError(st, "invalid serving form")
 
     def close(self):
         if getattr(self, "h", None):
@@ -472,6 +485,6 @@ class Server:
         return res.value, lat.value, br.value, (bufs[1] if bufs is not None else None)
 
     def stats(self):
-        v = np.zeros(12)
-        load().aifmm_server_stats(self.h, _dp(v), 12)
+        v = np.zeros(len(self.STAT_KEYS))
+        load().aifmm_server_stats(self.h, _dp(v), len(self.STAT_KEYS))
         return dict(zip(self.STAT_KEYS, v.tolist()))

@@ -35,52 +35,68 @@ struct AcaJob {
 };
 
 // ---- dense
+// The factorisation kernels serve both forms: complex128 blocks (the plain
+// form) and complex64 blocks (the mixed form).  Their descriptors hold untyped
+// element pointers; each launcher takes the element size es (16 or 8 bytes)
+// of its whole batch.  Scalars (alpha, beta, thresholds) are always double.
 struct QRJob {
-  double2* a; int lda;
+  void* a; int lda;
   int m, n;
-  double2* tau;
+  void* tau;
   int* perm;
-  double* norms;     // 2n
+  double* norms;     // 2n reals of the element's real type
   double thr;        // 0 -> min(m,n)*eps
   int* info;         // [0] nonzero pivots, [1] rank
   double* maxpiv;
 };
 
 struct SolveJob {        // X = alpha * QR^{-1} B
-  const double2* qr; int ldq; int m, n;
-  const double2* tau; const int* perm; const int* info;
-  const double2* B; int ldb;   // nullptr -> identity
-  double2* X; int ldx;
+  const void* qr; int ldq; int m, n;
+  const void* tau; const int* perm; const int* info;
+  const void* B; int ldb;   // nullptr -> identity
+  void* X; int ldx;
   int nrhs;
   double2 alpha;
-  double2* work;         // m x nrhs
+  void* work;            // m x nrhs
 };
 
 struct FormQJob {
-  const double2* qr; int ldq; int m, n;
-  const double2* tau;
-  double2* Q; int ldQ;
+  const void* qr; int ldq; int m, n;
+  const void* tau;
+  void* Q; int ldQ;
   const int* ncols_dev;
   int ncols;             // < 0 -> read ncols_dev[0]
 };
 
 struct GemmTerm {        // op(A) (m x k) * op(B) (k x n); op 0 = N, 1 = conjugate transpose
-  const double2* A; const double2* B;
+  const void* A; const void* B;
   int lda, ldb, opA, opB, k;
 };
 struct GemmDesc {        // C = alpha * sum_t op(A_t) op(B_t) + beta * C
-  double2* C; int ldc; int m, n;
+  void* C; int ldc; int m, n;
   double2 alpha, beta;
   int term0, nterms;
 };
 
-struct GeamDesc {        // C = alpha op(A) + beta C
-  const double2* A; double2* C;
+// C = alpha op(A) + beta C; A and C may differ in element size (the copies
+// between the complex128 assembly and complex64 factors convert)
+struct GeamDesc {
+  const void* A; void* C;
   int lda, ldc, opA, m, n;
+  int esA, esC;
   double2 alpha, beta;
+  const double* rs;      // optional (nullptr: 1): C(i, j) = alpha rs[i] op(A)(i, j) cs[j] + beta C(i, j)
+  const double* cs;
 };
 
-struct NormDesc { const double2* A; int lda, m, n; double* out; };
+// Frobenius norm of a block of either element size, accumulated in double
+struct NormDesc { const void* A; int lda, m, n; int es; double* out; };
+
+// Equilibration of a complex128 block: mode 0, the column norms of diag(scale) A
+// (scale over rows, may be nullptr); mode 1, the row norms of A diag(scale)
+// (scale over columns).  s = 1 / norm and is = norm per column (row); a zero
+// norm gives s = is = 1.
+struct EquilDesc { const double2* A; int lda, m, n; int mode; const double* scale; double* s; double* is; };
 
 struct SkelLUJob {       // X = D^{-1} B, D = A(rows, cols) or its adjoint
   const int* rows; const int* cols; int r;
@@ -97,21 +113,21 @@ struct SkelLUJob {       // X = D^{-1} B, D = A(rows, cols) or its adjoint
 // R' = nL^H P2P_kb, R = nL^H L2P_k; row QR of [P2M_b^H | R'^H] -> rank rr,
 // nPt = Q(:, :rr); M2L' = R M2L_kb (nPt^H P2M_b^H)^H + (nPt^H R'^H)^H.
 struct CompressJob {
-  const double2* L2P; int ldL;     // m x rK
-  const double2* Pkb; int ldP;     // m x c
-  const double2* P2M; int ldM;     // rb x c
-  const double2* M2L; int ldT;     // rK x rb
+  const void* L2P; int ldL;        // m x rK
+  const void* Pkb; int ldP;        // m x c
+  const void* P2M; int ldM;        // rb x c
+  const void* M2L; int ldT;        // rK x rb
   int m, rK, c, rb;
   double tol;
-  double2* nL;                     // out: m x rc (ld m), room for min(m, rK + c) columns
-  double2* nPt;                    // out: c x rr (ld c), room for min(c, rb + min(m, rK + c)) columns
-  double2* M2Lo; int ldO;          // out: rc x rr
+  void* nL;                        // out: m x rc (ld m), room for min(m, rK + c) columns
+  void* nPt;                       // out: c x rr (ld c), room for min(c, rb + min(m, rK + c)) columns
+  void* M2Lo; int ldO;             // out: rc x rr
   int* ranks;                      // out: rc, rr
   // scratch
-  double2* Acol;                   // m x (rK + c)
-  double2* Arow;                   // c x (rb + rc)
-  double2* tau; int* perm; int* info;
-  double2* Rkp; double2* Rk; double2* Rn; double2* Rnp; double2* Tm;
+  void* Acol;                      // m x (rK + c)
+  void* Arow;                      // c x (rb + rc)
+  void* tau; int* perm; int* info;
+  void* Rkp; void* Rk; void* Rn; void* Rnp; void* Tm;
 };
 
 // launchers (return a cudaError_t value)
@@ -128,22 +144,24 @@ int aifmm_launch_dense_matvec(const double2* x, double2* y, int N, int nrhs, con
 int aifmm_launch_green_matvec_add(const double2* x, double2* y, int N, int nrhs, const EntryCtx& ctx,
                                   cudaStream_t stream);
 int aifmm_launch_aca(const AcaJob* d_jobs, int njobs, double tol, const EntryCtx& ctx, cudaStream_t stream);
-int aifmm_launch_qr_factor(const QRJob* d_jobs, int njobs, cudaStream_t s);
-int aifmm_launch_qr_solve(const SolveJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s);
-size_t aifmm_qr_smem_bytes(int m, int n);
+int aifmm_launch_qr_factor(const QRJob* d_jobs, int njobs, int es, cudaStream_t s);
+int aifmm_launch_qr_solve(const SolveJob* d_jobs, const int* d_col_off, int njobs, int total_cols, int es,
+                          cudaStream_t s);
+size_t aifmm_qr_smem_bytes(int m, int n, int es);
 // one warp per right-hand side (8 per CTA), the column in registers; m <= 224 and
 // the factor's first nzp columns must fit in shared memory
 int aifmm_launch_qr_solve_warp(const SolveJob* d_jobs, const int* d_cta_off, int njobs, int total_ctas, int mmax,
-                               int nzpmax, cudaStream_t s);
+                               int nzpmax, int es, cudaStream_t s);
 // one CTA per factorisation, the matrix in shared memory (aifmm_qr_smem_bytes)
-int aifmm_launch_qr_factor_smem(const QRJob* d_jobs, int njobs, size_t smem, cudaStream_t s);
+int aifmm_launch_qr_factor_smem(const QRJob* d_jobs, int njobs, size_t smem, int es, cudaStream_t s);
 // shared memory the fused compression needs for these sizes (0: does not fit)
-size_t aifmm_compress_smem_bytes(int m, int rK, int c, int rb);
-int aifmm_launch_compress_p2p(const CompressJob* d_jobs, int njobs, size_t smem, cudaStream_t s);
-int aifmm_launch_formq(const FormQJob* d_jobs, const int* d_col_off, int njobs, int total_cols, cudaStream_t s);
+size_t aifmm_compress_smem_bytes(int m, int rK, int c, int rb, int es);
+int aifmm_launch_compress_p2p(const CompressJob* d_jobs, int njobs, size_t smem, int es, cudaStream_t s);
+int aifmm_launch_formq(const FormQJob* d_jobs, const int* d_col_off, int njobs, int total_cols, int es, cudaStream_t s);
 // tile_cols: output tile width, 32 (32 x 32 tiles) or 16 (32 x 16 tiles for thin products)
 int aifmm_launch_gemm(const GemmDesc* d, const GemmTerm* d_terms, const int* d_tile_off, int nd, int total_tiles,
-                      cudaStream_t s, int tile_cols);
+                      cudaStream_t s, int tile_cols, int es = 16);
 int aifmm_launch_geam(const GeamDesc* d, const long long* d_off, int nd, long long total, cudaStream_t s);
 int aifmm_launch_norms(const NormDesc* d, int nd, cudaStream_t s);
+int aifmm_launch_equilibrate(const EquilDesc* d, int nd, cudaStream_t s);
 int aifmm_launch_skel_lu(const SkelLUJob* d, int nd, const EntryCtx& ctx, cudaStream_t s);

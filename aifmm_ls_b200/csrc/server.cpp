@@ -19,7 +19,14 @@
 //     a result does not depend on the batch it rode in;
 //   * overlap: each worker drives its own handle and CUDA streams, so work on
 //     different keys runs concurrently on the GPU; one key is used by one worker
-//     at a time (a handle's calls must not overlap).
+//     at a time (a handle's calls must not overlap);
+//   * form (aifmm_server_set_form): plain -- FP64 factors, direct solves -- or
+//     mixed -- complex64 factors kept with the complex128 assembly, and every
+//     solve refined by GMRES against the compressed product to a relative
+//     residual.  A column's refined result does not depend on its batch beyond
+//     that tolerance (the columns iterate in lockstep until the worst converges).
+//     When the refinement stagnates (complex64 factors of a deep tree), the key
+//     is refactored in FP64 from its kept assembly and the batch refined again.
 // Failures (bad descriptions, a factorisation that cannot fit, CUDA errors) end
 // the request with a status; the server keeps running.
 #include <algorithm>
@@ -62,6 +69,9 @@ struct Req {
 struct Factor {
   aifmm_desc desc{};
   aifmm_problem* p = nullptr;
+  int precision = AIFMM_PRECISION_FP64;  // the precision of its factors
+  bool refine = false;                   // mixed form: every solve refined to rtol
+  double rtol = 0;
   bool ready = false;     // factors resident
   bool busy = false;      // a worker is using the handle
   bool queued_factor = false;  // a factorize request for it is waiting
@@ -95,6 +105,10 @@ struct aifmm_server {
   bool stopping = false;
   int factoring = 0;    // workers running a factorisation
   int factor_cap = -1;  // at most this many at once (< 0: all workers but one)
+  int precision = AIFMM_PRECISION_FP64;  // the form of factorisations admitted from now on
+  double rtol = 1e-8;
+  long refine_iters = 0;                 // GMRES iterations over all refined batches
+  long promotions = 0;                   // mixed-form keys refactored in FP64 (refinement stagnated)
   long next_id = 1;
   uint64_t tick = 0;
   // statistics
@@ -107,10 +121,13 @@ struct aifmm_server {
   // ~20 GB of ACA workspace during its assembly, ~65 KB per unknown in all,
   // scaled by the points per leaf.  Once factored, the measured footprint (the
   // workspace returned) replaces the estimate.
-  static size_t estimate(const aifmm_desc& d) {
+  // The mixed form holds the complex128 assembly next to the live blocks while it
+  // converts them to complex64: about 1.7 times that peak.
+  static size_t estimate(const aifmm_desc& d, int precision) {
     const double rank = (double)d.n_cheb * d.n_cheb;
     const double N = std::ldexp(1.0, 2 * d.depth) * rank;
-    return (size_t)(N * rank * 1800.0) + (size_t(64) << 20);
+    const double per = precision == AIFMM_PRECISION_C64 ? 3000.0 : 1800.0;
+    return (size_t)(N * rank * per) + (size_t(64) << 20);
   }
   size_t in_use() const {
     size_t s = 0;
@@ -162,7 +179,8 @@ struct aifmm_server {
     if ((st = aifmm_build_tree(p)) != AIFMM_OK) return fail(st);
     if ((st = aifmm_assemble(p)) != AIFMM_OK) return fail(st);
     if ((st = aifmm_autotune(p, nullptr, nullptr)) != AIFMM_OK) return fail(st);  // tile widths for this problem
-    if ((st = aifmm_factorize(p, AIFMM_PRECISION_FP64, 0)) != AIFMM_OK) return fail(st);
+    const int flags = f.precision == AIFMM_PRECISION_C64 ? AIFMM_KEEP_ASSEMBLY : 0;
+    if ((st = aifmm_factorize(p, f.precision, flags)) != AIFMM_OK) return fail(st);
     if ((st = aifmm_trim(p)) != AIFMM_OK) return fail(st);
     double v[15] = {0};
     aifmm_stats(p, v, 15);
@@ -190,7 +208,7 @@ struct aifmm_server {
         Req* r = *it;
         Factor& f = factors[r->key];
         if (f.busy) { ++it; continue; }
-        const size_t need = estimate(r->desc);
+        const size_t need = estimate(r->desc, precision);
         if (need > budget) {  // can never fit
           it = factor_q.erase(it);
           f.queued_factor = false;
@@ -231,7 +249,10 @@ struct aifmm_server {
       if (fr) {
         Factor& f = factors[fr->key];
         f.desc = fr->desc;
-        const size_t need = estimate(f.desc);
+        f.precision = precision;
+        f.refine = precision == AIFMM_PRECISION_C64;
+        f.rtol = rtol;
+        const size_t need = estimate(f.desc, f.precision);
         f.busy = true;
         f.reserve = need;
         ++factoring;
@@ -292,9 +313,34 @@ struct aifmm_server {
         std::memcpy(B.data() + o, r->b, sizeof(double) * 2 * (size_t)N * r->nrhs);
         o += (size_t)2 * N * r->nrhs;
       }
-      const aifmm_status st =
-          aifmm_solve(p, width, B.data(), N, X.data(), N, nullptr, AIFMM_PTR_HOST | AIFMM_SOLVE_GRAPH);
-      std::string err = st == AIFMM_OK ? "" : aifmm_last_error(p);
+      int iters = 0;
+      std::string err;
+      const bool refine = f.refine;
+      bool promoted = false;
+      aifmm_status st =
+          refine ? aifmm_solve_refined(p, width, B.data(), N, X.data(), N, f.rtol, 90, &iters, nullptr, AIFMM_PTR_HOST)
+                 : aifmm_solve(p, width, B.data(), N, X.data(), N, nullptr, AIFMM_PTR_HOST | AIFMM_SOLVE_GRAPH);
+      if (refine && st == AIFMM_ERR_NUMERIC && f.precision == AIFMM_PRECISION_C64) {
+        // complex64 factors that do not precondition this problem (a deep tree's
+        // growth times FP32 rounding): refactor from the kept complex128 assembly in
+        // FP64 and refine again; the key keeps the FP64 factors.  The refactoring
+        // is admitted like a factorisation (idle factors evicted to make room).
+        bool room;
+        {
+          std::lock_guard<std::mutex> g(mu);
+          room = make_room(estimate(f.desc, AIFMM_PRECISION_FP64), skey);
+        }
+        if (!room) {
+          st = AIFMM_ERR_NOMEM;
+          err = "no room to refactor in FP64 after the complex64 refinement stagnated";
+        } else {
+          st = aifmm_factorize(p, AIFMM_PRECISION_FP64, AIFMM_KEEP_ASSEMBLY);
+          if (st == AIFMM_OK)
+            st = aifmm_solve_refined(p, width, B.data(), N, X.data(), N, f.rtol, 90, &iters, nullptr, AIFMM_PTR_HOST);
+          promoted = true;
+        }
+      }
+      if (st != AIFMM_OK && err.empty()) err = aifmm_last_error(p);
       double v[15] = {0};
       aifmm_stats(p, v, 15);  // the graphs' buffers count towards the key's footprint
       o = 0;
@@ -304,11 +350,16 @@ struct aifmm_server {
           o += (size_t)2 * N * r->nrhs;
         }
       lk.lock();
+      if (promoted) {
+        f.precision = AIFMM_PRECISION_FP64;
+        ++promotions;
+      }
       f.busy = false;
       f.bytes = (size_t)(v[13] + v[14]);
       f.last_use = ++tick;
       ++batches;
       batch_rhs_total += tot;
+      refine_iters += iters;
       for (Req* r : batch) { r->batch_rhs = tot; finish(r, st, err); }
       cv_done.notify_all();
       cv_work.notify_all();
@@ -359,6 +410,15 @@ aifmm_status aifmm_server_set_factor_workers(aifmm_server* s, int n) {
   std::lock_guard<std::mutex> lk(s->mu);
   s->factor_cap = std::min(n, (int)s->workers.size());
   s->cv_work.notify_all();
+  return AIFMM_OK;
+}
+
+aifmm_status aifmm_server_set_form(aifmm_server* s, int precision, double rtol) {
+  if (!s || (precision != AIFMM_PRECISION_FP64 && precision != AIFMM_PRECISION_C64)) return AIFMM_ERR_ARG;
+  if (precision == AIFMM_PRECISION_C64 && !(rtol > 0 && rtol < 1)) return AIFMM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->precision = precision;
+  s->rtol = rtol;
   return AIFMM_OK;
 }
 
@@ -426,12 +486,13 @@ aifmm_status aifmm_server_stats(aifmm_server* s, double* out, int n) {
   std::lock_guard<std::mutex> lk(s->mu);
   int resident = 0;
   for (auto& kv : s->factors) resident += kv.second.ready ? 1 : 0;
-  const double v[12] = {percentile(s->lat_solve, 0.5), percentile(s->lat_solve, 0.99),
+  const double v[14] = {percentile(s->lat_solve, 0.5), percentile(s->lat_solve, 0.99),
                         percentile(s->lat_factor, 0.5), percentile(s->lat_factor, 0.99),
                         (double)s->lat_solve.size(), (double)s->lat_factor.size(), (double)s->evictions,
                         (double)s->batches, s->batches ? (double)s->batch_rhs_total / s->batches : 0.0,
-                        (double)s->in_use(), (double)resident, (double)s->rejected};
-  for (int i = 0; i < n && i < 12; ++i) out[i] = v[i];
+                        (double)s->in_use(), (double)resident, (double)s->rejected,
+                        s->batches ? (double)s->refine_iters / s->batches : 0.0, (double)s->promotions};
+  for (int i = 0; i < n && i < 14; ++i) out[i] = v[i];
   return AIFMM_OK;
 }
 

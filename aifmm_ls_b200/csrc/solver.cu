@@ -267,8 +267,29 @@ class GrowBuf {
   size_t cap_ = 0;
 };
 
+// A device pointer to complex elements of either form: es = 16 bytes
+// (complex128, the assembly and the plain factorisation) or 8 (complex64, the
+// factorisation of the mixed form).  Offsets count elements.
+struct EP {
+  char* b = nullptr;
+  int es = 16;
+  EP() = default;
+  EP(std::nullptr_t) {}
+  EP(double2* p) : b(reinterpret_cast<char*>(p)), es(16) {}
+  EP(const double2* p) : b(reinterpret_cast<char*>(const_cast<double2*>(p))), es(16) {}
+  EP(void* p, int es_) : b(static_cast<char*>(p)), es(es_) {}
+  EP operator+(size_t n) const { EP r = *this; if (b) r.b = b + n * (size_t)es; return r; }
+  explicit operator bool() const { return b != nullptr; }
+  void* v() const { return b; }
+  // the complex128 view, for the kernels that exist only in that form
+  double2* d() const {
+    if (b && es != 16) throw Fail(AIFMM_ERR_STATE, "a complex128 block was expected");
+    return reinterpret_cast<double2*>(b);
+  }
+};
+
 struct Blk {
-  double2* p = nullptr;
+  EP p;
   int r = 0, c = 0, ld = 0;
   size_t cap = 0;  // bytes owned from the pool (0: view or scratch)
   long size() const { return (long)r * c; }
@@ -276,7 +297,7 @@ struct Blk {
 
 struct QRF {
   Blk qr;
-  double2* tau = nullptr;
+  void* tau = nullptr;          // min(m, n) elements of the factor's type
   int* perm = nullptr;
   int* info = nullptr;
   double* norms = nullptr;
@@ -414,18 +435,25 @@ struct aifmm_problem {
   }
 
   // ------------------------------------------------------------------ blocks
-  Blk newblk(int r, int c) {
+  // Element size of the blocks that newblk / scr hand out: 16 (complex128)
+  // everywhere except while the mixed form factorises and solves (8, complex64).
+  int es_ = 16;
+  Blk newblk(int r, int c, int es = 0) {
+    if (es == 0) es = es_;
     Blk b; b.r = r; b.c = c; b.ld = r > 0 ? r : 1;
-    if ((long)r * c > 0) { b.cap = sizeof(double2) * (size_t)r * c; b.p = static_cast<double2*>(pool.alloc(b.cap)); }
+    b.p.es = es;
+    if ((long)r * c > 0) { b.cap = (size_t)es * r * c; b.p = EP(pool.alloc(b.cap), es); }
     return b;
   }
-  Blk scr(int r, int c) {
+  Blk scr(int r, int c, int es = 0) {
+    if (es == 0) es = es_;
     Blk b; b.r = r; b.c = c; b.ld = r > 0 ? r : 1;
-    if ((long)r * c > 0) b.p = static_cast<double2*>(scratch.get(sizeof(double2) * (size_t)r * c));
+    b.p.es = es;
+    if ((long)r * c > 0) b.p = EP(scratch.get((size_t)es * r * c), es);
     return b;
   }
   void drop(Blk& b) {
-    if (b.p && b.cap) pool.defer_free(b.p, b.cap);
+    if (b.p && b.cap) pool.defer_free(b.p.v(), b.cap);
     b = Blk();
   }
   void assign(Blk& dst, const Blk& src) { drop(dst); dst = src; }
@@ -496,11 +524,14 @@ struct aifmm_problem {
                                         " A " + std::to_string(A.r) + "x" + std::to_string(A.c) + " B " +
                                         std::to_string(B.r) + "x" + std::to_string(B.c));
     if (m == 0 || n == 0) return;
+    if (k > 0 && (A.p.es != C.p.es || B.p.es != C.p.es))
+      throw Fail(AIFMM_ERR_STATE, "gemm operands of different element sizes");
+    gemm_batch_es(C.p.es);
     GemmDesc g;
-    g.C = C.p; g.ldc = C.ld; g.m = m; g.n = n; g.alpha = alpha; g.beta = beta;
+    g.C = C.p.v(); g.ldc = C.ld; g.m = m; g.n = n; g.alpha = alpha; g.beta = beta;
     g.term0 = (int)gt.size(); g.nterms = 0;
     if (k > 0) {
-      GemmTerm t; t.A = A.p; t.B = B.p; t.lda = A.ld; t.ldb = B.ld; t.opA = opA; t.opB = opB; t.k = k;
+      GemmTerm t; t.A = A.p.v(); t.B = B.p.v(); t.lda = A.ld; t.ldb = B.ld; t.opA = opA; t.opB = opB; t.k = k;
       gt.push_back(t);
       g.nterms = 1;
     }
@@ -509,14 +540,16 @@ struct aifmm_problem {
   // C = beta C + alpha * sum_t A_t B_t
   void gemm_sum(const Blk& C, const std::vector<std::pair<Blk, Blk>>& terms, double2 alpha, double2 beta) {
     if (C.r == 0 || C.c == 0) return;
+    gemm_batch_es(C.p.es);
     GemmDesc g;
-    g.C = C.p; g.ldc = C.ld; g.m = C.r; g.n = C.c; g.alpha = alpha; g.beta = beta;
+    g.C = C.p.v(); g.ldc = C.ld; g.m = C.r; g.n = C.c; g.alpha = alpha; g.beta = beta;
     g.term0 = (int)gt.size(); g.nterms = 0;
     for (auto& pr : terms) {
       const Blk& A = pr.first; const Blk& B = pr.second;
       if (A.r != C.r || B.c != C.c || A.c != B.r) throw Fail(AIFMM_ERR_NUMERIC, "gemm_sum shape mismatch");
       if (A.c == 0) continue;
-      GemmTerm t; t.A = A.p; t.B = B.p; t.lda = A.ld; t.ldb = B.ld; t.opA = 0; t.opB = 0; t.k = A.c;
+      if (A.p.es != C.p.es || B.p.es != C.p.es) throw Fail(AIFMM_ERR_STATE, "gemm operands of different element sizes");
+      GemmTerm t; t.A = A.p.v(); t.B = B.p.v(); t.lda = A.ld; t.ldb = B.ld; t.opA = 0; t.opB = 0; t.k = A.c;
       gt.push_back(t);
       ++g.nterms;
     }
@@ -526,6 +559,12 @@ struct aifmm_problem {
   // whose products are all thin (n <= 16 columns, e.g. a block times the
   // right-hand sides), [1] otherwise
   int gemm_cols[2] = {32, 32};
+  // one element size per batch: a product of the other size flushes the batch first
+  int gemm_es = 16;
+  void gemm_batch_es(int es) {
+    if (!gd.empty() && gemm_es != es) flush_gemm();
+    gemm_es = es;
+  }
   void flush_gemm() {
     if (gd.empty()) { gt.clear(); return; }
     int nmax = 0;
@@ -546,8 +585,8 @@ struct aifmm_problem {
       const GemmDesc* d1 = static_cast<const GemmDesc*>(ptrs[1]);
       const GemmTerm* d0 = static_cast<const GemmTerm*>(ptrs[0]);
       const int* d2 = static_cast<const int*>(ptrs[2]);
-      const int nd = (int)gd.size();
-      KL(run_op([=](cudaStream_t s_) { return aifmm_launch_gemm(d1, d0, d2, nd, tot, s_, tc); }));
+      const int nd = (int)gd.size(), es = gemm_es;
+      KL(run_op([=](cudaStream_t s_) { return aifmm_launch_gemm(d1, d0, d2, nd, tot, s_, tc, es); }));
     }
     if (pr) prof_end(2, a, fl);
     gd.clear(); gt.clear();
@@ -556,7 +595,9 @@ struct aifmm_problem {
     const int m = opA ? A.c : A.r, n = opA ? A.r : A.c;
     if (C.r != m || C.c != n) throw Fail(AIFMM_ERR_NUMERIC, "geam shape mismatch");
     if (m == 0 || n == 0) return;
-    GeamDesc g; g.A = A.p; g.C = C.p; g.lda = A.ld; g.ldc = C.ld; g.opA = opA; g.m = m; g.n = n;
+    GeamDesc g; g.A = A.p.v(); g.C = C.p.v(); g.lda = A.ld; g.ldc = C.ld; g.opA = opA; g.m = m; g.n = n;
+    g.rs = nullptr; g.cs = nullptr;
+    g.esA = A.p.es; g.esC = C.p.es;
     g.alpha = alpha; g.beta = beta;
     ged.push_back(g);
   }
@@ -578,13 +619,13 @@ struct aifmm_problem {
   void zero(const Blk& b) {
     if (b.size() == 0) return;
     if (b.ld == b.r) {
-      double2* p_ = b.p;
-      const size_t n_ = sizeof(double2) * (size_t)b.r * b.c;
+      void* p_ = b.p.v();
+      const size_t n_ = (size_t)b.p.es * b.r * b.c;
       CK((cudaError_t)run_op([=](cudaStream_t s_) { return (int)cudaMemsetAsync(p_, 0, n_, s_); }));
     } else {
       for (int j = 0; j < b.c; ++j) {
-        double2* p_ = b.p + (size_t)j * b.ld;
-        const size_t n_ = sizeof(double2) * b.r;
+        void* p_ = (b.p + (size_t)j * b.ld).v();
+        const size_t n_ = (size_t)b.p.es * b.r;
         CK((cudaError_t)run_op([=](cudaStream_t s_) { return (int)cudaMemsetAsync(p_, 0, n_, s_); }));
       }
     }
@@ -600,28 +641,32 @@ struct aifmm_problem {
       f.cap[1] = sizeof(int) * std::max(1, n);
       f.cap[2] = sizeof(int) * 4;
       f.cap[3] = sizeof(double) * std::max(1, 2 * n);
-      f.tau = static_cast<double2*>(pool.alloc(f.cap[0]));
+      f.tau = pool.alloc(f.cap[0]);
       f.perm = static_cast<int*>(pool.alloc(f.cap[1]));
       f.info = static_cast<int*>(pool.alloc(f.cap[2]));
       f.norms = static_cast<double*>(pool.alloc(f.cap[3]));
     } else {
-      f.tau = static_cast<double2*>(scratch.get(sizeof(double2) * std::max(1, s)));
+      f.tau = scratch.get(sizeof(double2) * std::max(1, s));
       f.perm = static_cast<int*>(scratch.get(sizeof(int) * std::max(1, n)));
       f.info = static_cast<int*>(scratch.get(sizeof(int) * 4));
       f.norms = static_cast<double*>(scratch.get(sizeof(double) * std::max(1, 2 * n)));
     }
     f.valid = true;
-    QRJob q; q.a = A.p; q.lda = A.ld; q.m = A.r; q.n = A.c; q.tau = f.tau; q.perm = f.perm; q.norms = f.norms;
+    if (!qj.empty() && qr_es != A.p.es) flush_qr();
+    qr_es = A.p.es;
+    QRJob q; q.a = A.p.v(); q.lda = A.ld; q.m = A.r; q.n = A.c; q.tau = f.tau; q.perm = f.perm; q.norms = f.norms;
     q.thr = thr; q.info = f.info; q.maxpiv = nullptr;
     qj.push_back(q);
   }
+  int qr_es = 16, solve_es = 16, formq_es = 16;  // element size of each pending batch
   void flush_qr() {
     if (qj.empty()) return;
     std::vector<QRJob> small, large;
     size_t smem = 0;
     double fl_small = 0, fl_large = 0;
+    const int es = qr_es;
     for (auto& j : qj) {
-      const size_t b = aifmm_qr_smem_bytes(j.m, j.n);
+      const size_t b = aifmm_qr_smem_bytes(j.m, j.n, es);
       if (b <= size_t(200) << 10) { small.push_back(j); smem = std::max(smem, b); fl_small += qr_flops(j.m, j.n); }
       else { large.push_back(j); fl_large += qr_flops(j.m, j.n); }
     }
@@ -629,14 +674,14 @@ struct aifmm_problem {
       const QRJob* dq = stage.put(small, cur);
       cudaEvent_t a;
       const bool pr = prof_begin(0, a);
-      KL(aifmm_launch_qr_factor_smem(dq, (int)small.size(), smem, cur));
+      KL(aifmm_launch_qr_factor_smem(dq, (int)small.size(), smem, es, cur));
       if (pr) prof_end(0, a, fl_small);
     }
     if (!large.empty()) {
       const QRJob* dq = stage.put(large, cur);
       cudaEvent_t a;
       const bool pr = prof_begin(0, a);
-      KL(aifmm_launch_qr_factor(dq, (int)large.size(), cur));
+      KL(aifmm_launch_qr_factor(dq, (int)large.size(), es, cur));
       if (pr) prof_end(0, a, fl_large);
     }
     qj.clear();
@@ -647,8 +692,12 @@ struct aifmm_problem {
     if (!identity && B.r != f.qr.r) throw Fail(AIFMM_ERR_NUMERIC, "solve rhs rows mismatch");
     if (X.r != f.qr.c || X.c != nr) throw Fail(AIFMM_ERR_NUMERIC, "solve output shape mismatch");
     if (nr == 0 || X.r == 0) return;
-    SolveJob s; s.qr = f.qr.p; s.ldq = f.qr.ld; s.m = f.qr.r; s.n = f.qr.c; s.tau = f.tau; s.perm = f.perm;
-    s.info = f.info; s.B = identity ? nullptr : B.p; s.ldb = identity ? 1 : B.ld; s.X = X.p; s.ldx = X.ld;
+    const int es = f.qr.p.es;
+    if (X.p.es != es || (!identity && B.p.es != es)) throw Fail(AIFMM_ERR_STATE, "solve operands of different element sizes");
+    if (!sj.empty() && solve_es != es) flush_solve();
+    solve_es = es;
+    SolveJob s; s.qr = f.qr.p.v(); s.ldq = f.qr.ld; s.m = f.qr.r; s.n = f.qr.c; s.tau = f.tau; s.perm = f.perm;
+    s.info = f.info; s.B = identity ? nullptr : B.p.v(); s.ldb = identity ? 1 : B.ld; s.X = X.p.v(); s.ldx = X.ld;
     s.nrhs = nr; s.alpha = alpha;
     s.work = nullptr;
     sj.push_back(s);
@@ -659,9 +708,10 @@ struct aifmm_problem {
     // column in registers; larger systems (the base level): the global-memory kernel
     std::vector<SolveJob> small, large;
     int mmax = 1, nmax = 1;
+    const int es = solve_es;
     for (auto& j : sj) {
       const int s_ = std::min(j.m, j.n);
-      const size_t need = sizeof(double2) * ((size_t)(j.m | 1) * s_ + 2 * (size_t)s_);
+      const size_t need = (size_t)es * ((size_t)(j.m | 1) * s_ + (size_t)s_) + sizeof(double2) * s_;
       if (j.m <= 224 && need <= (size_t(200) << 10)) {
         small.push_back(j);
         mmax = std::max(mmax, j.m);
@@ -670,7 +720,7 @@ struct aifmm_problem {
         large.push_back(j);
       }
     }
-    if (sizeof(double2) * ((size_t)(mmax | 1) * nmax + 2 * (size_t)nmax) > (size_t(200) << 10)) {
+    if ((size_t)es * ((size_t)(mmax | 1) * nmax + (size_t)nmax) + sizeof(double2) * nmax > (size_t(200) << 10)) {
       // the batch's largest m and rank do not fit together: split by size
       for (auto& j : small) large.push_back(j);
       small.clear();
@@ -688,7 +738,7 @@ struct aifmm_problem {
         const SolveJob* d0 = static_cast<const SolveJob*>(ptrs[0]);
         const int* d1 = static_cast<const int*>(ptrs[1]);
         const int nj = (int)small.size();
-        KL(run_op([=](cudaStream_t s_) { return aifmm_launch_qr_solve_warp(d0, d1, nj, tot, mmax, nmax, s_); }));
+        KL(run_op([=](cudaStream_t s_) { return aifmm_launch_qr_solve_warp(d0, d1, nj, tot, mmax, nmax, es, s_); }));
       }
       if (pr) prof_end(1, a, fl);
     }
@@ -698,7 +748,7 @@ struct aifmm_problem {
       for (size_t i = 0; i < large.size(); ++i) {
         off[i] = tot;
         tot += large[i].nrhs;
-        large[i].work = static_cast<double2*>(scratch.get(sizeof(double2) * (size_t)large[i].m * large[i].nrhs));
+        large[i].work = scratch.get((size_t)es * large[i].m * large[i].nrhs);
       }
       auto ptrs = put_many_({{large.data(), large.size() * sizeof(SolveJob)}, {off.data(), off.size() * sizeof(int)}});
       double fl = 0;
@@ -709,7 +759,7 @@ struct aifmm_problem {
         const SolveJob* d0 = static_cast<const SolveJob*>(ptrs[0]);
         const int* d1 = static_cast<const int*>(ptrs[1]);
         const int nj = (int)large.size();
-        KL(run_op([=](cudaStream_t s_) { return aifmm_launch_qr_solve(d0, d1, nj, tot, s_); }));
+        KL(run_op([=](cudaStream_t s_) { return aifmm_launch_qr_solve(d0, d1, nj, tot, es, s_); }));
       }
       if (pr) prof_end(1, a, fl);
     }
@@ -717,7 +767,10 @@ struct aifmm_problem {
   }
   void formq(const QRF& f, const Blk& Q) {
     if (Q.size() == 0) return;
-    FormQJob j; j.qr = f.qr.p; j.ldq = f.qr.ld; j.m = f.qr.r; j.n = f.qr.c; j.tau = f.tau; j.Q = Q.p; j.ldQ = Q.ld;
+    if (Q.p.es != f.qr.p.es) throw Fail(AIFMM_ERR_STATE, "formq operands of different element sizes");
+    if (!fq.empty() && formq_es != Q.p.es) flush_formq();
+    formq_es = Q.p.es;
+    FormQJob j; j.qr = f.qr.p.v(); j.ldq = f.qr.ld; j.m = f.qr.r; j.n = f.qr.c; j.tau = f.tau; j.Q = Q.p.v(); j.ldQ = Q.ld;
     j.ncols_dev = nullptr; j.ncols = Q.c;
     fq.push_back(j);
   }
@@ -728,7 +781,7 @@ struct aifmm_problem {
     for (size_t i = 0; i < fq.size(); ++i) { off[i] = tot; tot += fq[i].ncols; }
     auto ptrs = stage.put_many({{fq.data(), fq.size() * sizeof(FormQJob)}, {off.data(), off.size() * sizeof(int)}}, cur);
     KL(aifmm_launch_formq(static_cast<const FormQJob*>(ptrs[0]), static_cast<const int*>(ptrs[1]), (int)fq.size(),
-                          tot, cur));
+                          tot, formq_es, cur));
     fq.clear();
   }
   void flush_all() { flush_geam(); flush_qr(); flush_solve(); flush_formq(); flush_gemm(); }
@@ -907,6 +960,7 @@ struct aifmm_problem {
 
   // ------------------------------------------------------------------ tree
   void build_tree() {
+    es_ = 16;
     auto t0 = std::chrono::steady_clock::now();
     release_tree();
     T.assign(depth + 1, {});
@@ -972,6 +1026,7 @@ struct aifmm_problem {
   }
 
   void assemble() {
+    es_ = 16;
     if (!tables_ready) throw Fail(AIFMM_ERR_STATE, "tables not computed or set");
     if (!tree_ready) throw Fail(AIFMM_ERR_STATE, "tree not built");
     auto t0 = std::chrono::steady_clock::now();
@@ -1084,8 +1139,8 @@ struct aifmm_problem {
         J.prim_bases = d_bases + ro[t];
         J.sec_bases = d_bases + ro[t] + rmax;
         Box& B = T[j][k];
-        if (outgoing) { drop(B.Ar); B.Ar = newblk(rmax, n2); J.out = B.Ar.p; B.Ar.ld = std::max(rmax, 1); }
-        else { drop(B.Ac); B.Ac = newblk(n1, rmax); J.out = B.Ac.p; }
+        if (outgoing) { drop(B.Ar); B.Ar = newblk(rmax, n2); J.out = B.Ar.p.d(); B.Ar.ld = std::max(rmax, 1); }
+        else { drop(B.Ac); B.Ac = newblk(n1, rmax); J.out = B.Ac.p.d(); }
       }
       st_asm_lists_ms += since(ta);
       ta = clk::now();
@@ -1165,13 +1220,13 @@ struct aifmm_problem {
         if (r == 0) continue;
         SkelLUJob a;  // L2P = Ac(:, :r) D1^{-1}, via LU of D1^H (F:1117-1119)
         a.rows = d_sk + lui[2 * k].rows; a.cols = d_sk + lui[2 * k].cols; a.r = r; a.adjD = 1;
-        a.B = B.Ac.p; a.ldb = B.Ac.ld; a.adjB = 1; a.m = m_in; a.X = B.L2P.p; a.ldx = B.L2P.ld; a.adjX = 1;
+        a.B = B.Ac.p.d(); a.ldb = B.Ac.ld; a.adjB = 1; a.m = m_in; a.X = B.L2P.p.d(); a.ldx = B.L2P.ld; a.adjX = 1;
         lwo.push_back(lws);
         lws += (sizeof(double2) * ((size_t)r * r + (size_t)r * m_in) + sizeof(int) * r + 511) & ~size_t(255);
         lj.push_back(a);
         SkelLUJob b;  // P2M = D2^{-1} Ar(:r, :) (F:1124-1126)
         b.rows = d_sk + lui[2 * k + 1].rows; b.cols = d_sk + lui[2 * k + 1].cols; b.r = r; b.adjD = 0;
-        b.B = B.Ar.p; b.ldb = B.Ar.ld; b.adjB = 0; b.m = m_out; b.X = B.P2M.p; b.ldx = B.P2M.ld; b.adjX = 0;
+        b.B = B.Ar.p.d(); b.ldb = B.Ar.ld; b.adjB = 0; b.m = m_out; b.X = B.P2M.p.d(); b.ldx = B.P2M.ld; b.adjX = 0;
         lwo.push_back(lws);
         lws += (sizeof(double2) * ((size_t)r * r + (size_t)r * m_out) + sizeof(int) * r + 511) & ~size_t(255);
         lj.push_back(b);
@@ -1213,7 +1268,7 @@ struct aifmm_problem {
             Blk m2l = newblk((int)B.in_check.size(), (int)O.out_charge.size());
             assign(B.M2L[kIL], m2l);
             if (m2l.size() == 0) return;
-            BlockDesc x; x.rows = nullptr; x.cols = nullptr; x.nr = m2l.r; x.nc = m2l.c; x.out = m2l.p;
+            BlockDesc x; x.rows = nullptr; x.cols = nullptr; x.nr = m2l.r; x.nc = m2l.c; x.out = m2l.p.d();
             x.ldo = m2l.ld; x.adjoint = 0;
             bd.push_back(x); rof.push_back(ic[k]); cof.push_back(oc[kIL]);
           };
@@ -1229,7 +1284,7 @@ struct aifmm_problem {
           Blk p = newblk(rank, rank);
           assign(B.P2P[nn], p);
           BlockDesc x; x.rows = d_iota + (size_t)k * rank; x.cols = d_iota + (size_t)nn * rank; x.nr = rank;
-          x.nc = rank; x.out = p.p; x.ldo = rank; x.adjoint = 0;
+          x.nc = rank; x.out = p.p.d(); x.ldo = rank; x.adjoint = 0;
           bd.push_back(x);
         };
         for (int n = 0; n < 8; ++n) if (B.nb[n] != -1) add(B.nb[n]);
@@ -1267,7 +1322,7 @@ struct aifmm_problem {
     if ((int)cands.size() >= norm_cap) throw Fail(AIFMM_ERR_NUMERIC, "too many fill-in candidates");
     // every slot is written by a norm kernel (an empty block gives 0), so all
     // writes to the slots are ordered by the stream
-    NormDesc n; n.A = b.p; n.lda = std::max(b.ld, 1); n.m = b.size() ? b.r : 0; n.n = b.size() ? b.c : 0;
+    NormDesc n; n.A = b.p.v(); n.es = b.p.es; n.lda = std::max(b.ld, 1); n.m = b.size() ? b.r : 0; n.n = b.size() ? b.c : 0;
     n.out = d_norms + cands.size();
     cands.push_back({kind, nn, pp});
     ndv.push_back(n);
@@ -1531,7 +1586,7 @@ struct aifmm_problem {
       if (Pkb.r != K.L2P.r) throw Fail(AIFMM_ERR_NUMERIC, "compress_P2P: block rows mismatch");
       if (Bb.P2M.c != Pkb.c || m2l.r != K.L2P.c || m2l.c != Bb.P2M.r)
         throw Fail(AIFMM_ERR_NUMERIC, "compress_P2P: block shapes");
-      const size_t need = aifmm_compress_smem_bytes(K.L2P.r, K.L2P.c, Pkb.c, Bb.P2M.r);
+      const size_t need = aifmm_compress_smem_bytes(K.L2P.r, K.L2P.c, Pkb.c, Bb.P2M.r, es_);
       if (need == 0) return false;
       smem = std::max(smem, need);
     }
@@ -1551,15 +1606,17 @@ struct aifmm_problem {
       out[s]->nPt = newblk(c, rrmax[s]);
       out[s]->M2L = scr(rcmax[s], rrmax[s]);
       CompressJob& J = jobs[s];
-      J.L2P = K.L2P.p; J.ldL = K.L2P.ld;
-      J.Pkb = Pkb.p; J.ldP = Pkb.ld;
-      J.P2M = Bb.P2M.p; J.ldM = Bb.P2M.ld;
-      J.M2L = m2l.p; J.ldT = m2l.ld;
+      for (const Blk* x : std::initializer_list<const Blk*>{&K.L2P, &Pkb, &Bb.P2M, &m2l})
+        if (x->size() && x->p.es != es_) throw Fail(AIFMM_ERR_STATE, "compress_P2P: block of the other form");
+      J.L2P = K.L2P.p.v(); J.ldL = K.L2P.ld;
+      J.Pkb = Pkb.p.v(); J.ldP = Pkb.ld;
+      J.P2M = Bb.P2M.p.v(); J.ldM = Bb.P2M.ld;
+      J.M2L = m2l.p.v(); J.ldT = m2l.ld;
       J.m = m; J.rK = rK; J.c = c; J.rb = rb; J.tol = tol_factor;
-      J.nL = out[s]->nL.p; J.nPt = out[s]->nPt.p;
-      J.M2Lo = out[s]->M2L.p; J.ldO = out[s]->M2L.ld;
+      J.nL = out[s]->nL.p.v(); J.nPt = out[s]->nPt.p.v();
+      J.M2Lo = out[s]->M2L.p.v(); J.ldO = out[s]->M2L.ld;
       J.ranks = ranks + 2 * s;
-      auto cg = [&](long elems) { return static_cast<double2*>(scratch.get(sizeof(double2) * std::max(1L, elems))); };
+      auto cg = [&](long elems) { return scratch.get((size_t)es_ * std::max(1L, elems)); };
       J.Acol = cg((long)m * n1);
       J.Arow = cg((long)c * n2max);
       J.tau = cg(std::max(rcmax[s], rrmax[s]));
@@ -1573,7 +1630,7 @@ struct aifmm_problem {
     }
     flush_all();
     const CompressJob* dj = stage.put(jobs, st);
-    KL(aifmm_launch_compress_p2p(dj, 2, smem, st));
+    KL(aifmm_launch_compress_p2p(dj, 2, smem, es_, st));
     sync();
     int rk[4];
     d2h(rk, ranks, sizeof rk);
@@ -2274,21 +2331,41 @@ struct aifmm_problem {
   long launches_factor = 0, launches_solve = 0;
   // eliminate_phase_efficient with the base-level factorisation (F:2407-2485),
   // right-hand side not carried
-  void factorize(int flags) {
+  // The mixed form factorises in complex64: its recompressions cannot resolve
+  // ranks below this relative tolerance (a few units of FP32 rounding of a
+  // 36-row block), so a tighter factor tolerance is raised to it.
+  static constexpr double kC64MinTol = 1e-6;
+  int factor_es = 16;
+  void factorize(int flags, int precision = AIFMM_PRECISION_FP64) {
     if (!assembled) throw Fail(AIFMM_ERR_STATE, "assemble() must run before factorize()");
     if (consumed && !have_saved)
       throw Fail(AIFMM_ERR_STATE, "the assembly was consumed by a previous factorisation: assemble again, or pass AIFMM_KEEP_ASSEMBLY");
     auto t0 = std::chrono::steady_clock::now();
     const long l0 = launches_;
+    release_plans();
     // the elimination consumes the assembled blocks; with AIFMM_KEEP_ASSEMBLY a
     // pristine copy is kept so that the handle can be factored again
+    es_ = 16;  // the kept assembly is restored in complex128, then converted
     if ((flags & AIFMM_KEEP_ASSEMBLY) || have_saved) snapshot_restore();
+    if (precision == AIFMM_PRECISION_C64) {
+      es_ = 8;
+      to_working_form();
+    }
     release_solve_state();
     factored = false;
     consumed = true;
+    factor_es = es_;
+    const double tol_keep = tol_factor;
+    if (es_ == 8) tol_factor = std::max(tol_factor, kC64MinTol);
     st_sync_ms = st_compress_ms = st_elim_ms = st_pending_ms = 0;
     st_syncs = st_compress = 0;
-    eliminate_phase_efficient();
+    try {
+      eliminate_phase_efficient();
+    } catch (...) {
+      tol_factor = tol_keep;
+      throw;
+    }
+    tol_factor = tol_keep;
     fwd_waves.assign(depth + 1, {});
     bwd_waves.assign(depth + 1, {});
     for (int j = 2; j <= depth; ++j) {
@@ -2511,7 +2588,7 @@ struct aifmm_problem {
     for (auto& lv : T)
       for (auto& B : lv) {
         for (Blk* b : {&B.sr, &B.sxb, &B.sy, &B.smr, &B.particles, &B.locals, &B.multipoles}) {
-          if (b->p && b->cap) pl.owned.push_back({b->p, b->cap});
+          if (b->p && b->cap) pl.owned.push_back({b->p.v(), b->cap});
           *b = Blk();
         }
       }
@@ -2574,8 +2651,8 @@ struct aifmm_problem {
       }
       mo[j][nBoxes[j]] = mt;
       lo[j][nBoxes[j]] = lt;
-      Mv[j] = scr(mt, nr);
-      Lv[j] = scr(lt, nr);
+      Mv[j] = scr(mt, nr, 16);
+      Lv[j] = scr(lt, nr, 16);
     }
     auto rows = [&](const Blk& v, int r0, int r1) { return Blk{v.p ? v.p + r0 : nullptr, r1 - r0, nr, v.ld}; };
     // upward: multipoles
@@ -2691,9 +2768,9 @@ struct aifmm_problem {
     std::vector<double> bn(nr);
     for (int c = 0; c < nr; ++c) bn[c] = std::sqrt(d[c].x) > 0 ? std::sqrt(d[c].x) : 1.0;
     precond(B, X);  // the direct solve is the starting guess
-    int it = 0;
-    double worst = 0;
-    for (;;) {
+    int it = 0, cycle = 0;
+    double worst = 0, worst_prev = 0;
+    for (;; ++cycle) {
       // true residual r = b - A_c x into V_0
       compressed_matvec(X, N, W, N, nr);
       CK(cudaMemcpyAsync(Vi(0), B, vb, cudaMemcpyDeviceToDevice, st));
@@ -2703,6 +2780,18 @@ struct aifmm_problem {
       worst = 0;
       for (int c = 0; c < nr; ++c) { beta[c] = std::sqrt(d[c].x); worst = std::max(worst, beta[c] / bn[c]); }
       if (worst <= rtol || it >= maxit) break;
+      // A cycle that does not halve the true residual means the preconditioner is
+      // not the linear operator GMRES assumes (complex64 factors of a deep tree:
+      // the elimination's internal growth times FP32 rounding): stop rather than
+      // iterate to maxit.
+      if (cycle > 0 && !(worst <= 0.5 * worst_prev)) {
+        gm_iters = it;
+        gm_relres = worst;
+        throw Fail(AIFMM_ERR_NUMERIC, "GMRES refinement stagnates: relative residual " + std::to_string(worst) +
+                                          " after " + std::to_string(it) + " iterations (the factors are not an "
+                                          "effective preconditioner)");
+      }
+      worst_prev = worst;
       {
         std::vector<double2> sc(nr);
         for (int c = 0; c < nr; ++c) sc[c] = make_double2(beta[c] > 0 ? 1.0 / beta[c] : 0.0, 0.0);
@@ -2713,8 +2802,11 @@ struct aifmm_problem {
       std::vector<std::vector<double>> cs(nr, std::vector<double>(m));
       std::vector<std::vector<double2>> sn(nr, std::vector<double2>(m)), g(nr, std::vector<double2>(m + 1, C0));
       for (int c = 0; c < nr; ++c) g[c][0] = make_double2(beta[c], 0.0);
+      // with complex64 factors the first cycle is short, so that a stagnating
+      // refinement is noticed early
+      const int mk = cycle == 0 && factor_es == 8 ? std::min(m, 10) : m;
       int k = 0;
-      for (; k < m && it < maxit; ++k, ++it) {
+      for (; k < mk && it < maxit; ++k, ++it) {
         precond(Vi(k), Z);
         compressed_matvec(Z, N, W, N, nr);
         for (int l = 0; l <= k; ++l) {  // modified Gram-Schmidt
@@ -2805,6 +2897,93 @@ struct aifmm_problem {
     saved.clear();
     pool.commit_frees();
   }
+  // The live (to be eliminated) blocks in complex64 for the mixed form.  The
+  // interpolative bases carry the contrast's dynamic range: a column of
+  // L2P = A(rows, skel) D^-1 scales with 1 / q(skeleton point), up to about
+  // 1 / tolerance in the far corners of a Gaussian contrast, which FP32 cannot
+  // carry next to O(1) entries.  So the conversion first equilibrates the
+  // compressed representation by a diagonal similarity transform of every box's
+  // local and multipole spaces -- locals l = S l', multipoles m' = T m, with
+  // S = diag(sigma), T = diag(tau) -- chosen bottom-up so that every L2P has unit
+  // columns and every P2M unit rows:
+  //   L2P' = S_children^-1 L2P S,  P2M' = T P2M T_children^-1,  M2L' = S_k^-1 M2L T_j^-1,
+  // (no children factor at the leaves; the leaf particle space and the leaf P2P
+  // blocks are unchanged, so right-hand sides and solutions need no scaling).
+  void to_working_form() {
+    if (es_ == 16) return;
+    std::vector<std::vector<long>> loff(depth + 2), moff(depth + 2);
+    long totL = 0, totM = 0;
+    for (int j = 2; j <= depth; ++j) {
+      loff[j].resize(nBoxes[j] + 1);
+      moff[j].resize(nBoxes[j] + 1);
+      for (int k = 0; k < nBoxes[j]; ++k) {
+        loff[j][k] = totL; totL += T[j][k].NumL;
+        moff[j][k] = totM; totM += T[j][k].NumM;
+      }
+      loff[j][nBoxes[j]] = totL;
+      moff[j][nBoxes[j]] = totM;
+    }
+    Tmp tS(this, sizeof(double) * 2 * std::max(1L, totL)), tT(this, sizeof(double) * 2 * std::max(1L, totM));
+    double* sig = tS.as<double>();
+    double* isig = sig + std::max(1L, totL);
+    double* tau = tT.as<double>();
+    double* itau = tau + std::max(1L, totM);
+    for (int j = depth; j >= 2; --j) {
+      std::vector<EquilDesc> ed;
+      for (int k = 0; k < nBoxes[j]; ++k) {
+        Box& B = T[j][k];
+        if (B.L2P.p.es != 16 || B.P2M.p.es != 16) throw Fail(AIFMM_ERR_STATE, "equilibration needs the complex128 bases");
+        if (B.L2P.c != B.NumL || B.P2M.r != B.NumM) throw Fail(AIFMM_ERR_NUMERIC, "equilibration: basis shapes");
+        if (j < depth && (B.L2P.r != loff[j + 1][4 * k + 4] - loff[j + 1][4 * k] ||
+                          B.P2M.c != moff[j + 1][4 * k + 4] - moff[j + 1][4 * k]))
+          throw Fail(AIFMM_ERR_NUMERIC, "equilibration: children's spaces");
+        if (B.L2P.size()) {
+          EquilDesc e; e.A = B.L2P.p.d(); e.lda = B.L2P.ld; e.m = B.L2P.r; e.n = B.L2P.c; e.mode = 0;
+          e.scale = j < depth ? isig + loff[j + 1][4 * k] : nullptr;
+          e.s = sig + loff[j][k]; e.is = isig + loff[j][k];
+          ed.push_back(e);
+        } else if (B.NumL > 0) {
+          throw Fail(AIFMM_ERR_NUMERIC, "equilibration: empty L2P with locals");
+        }
+        if (B.P2M.size()) {
+          EquilDesc e; e.A = B.P2M.p.d(); e.lda = B.P2M.ld; e.m = B.P2M.r; e.n = B.P2M.c; e.mode = 1;
+          e.scale = j < depth ? itau + moff[j + 1][4 * k] : nullptr;
+          e.s = tau + moff[j][k]; e.is = itau + moff[j][k];
+          ed.push_back(e);
+        } else if (B.NumM > 0) {
+          throw Fail(AIFMM_ERR_NUMERIC, "equilibration: empty P2M with multipoles");
+        }
+      }
+      if (!ed.empty()) {
+        const EquilDesc* d = stage.put(ed, st);
+        KL(aifmm_launch_equilibrate(d, (int)ed.size(), st));
+      }
+    }
+    auto conv = [&](Blk& b, const double* rs, const double* cs) {
+      if (b.size() == 0) { b.p.es = es_; return; }
+      Blk t = newblk(b.r, b.c);
+      GeamDesc g; g.A = b.p.v(); g.C = t.p.v(); g.lda = b.ld; g.ldc = t.ld; g.opA = 0; g.m = b.r; g.n = b.c;
+      g.esA = b.p.es; g.esC = t.p.es; g.alpha = C1; g.beta = C0; g.rs = rs; g.cs = cs;
+      ged.push_back(g);
+      assign(b, t);
+    };
+    for (int j = 2; j <= depth; ++j)
+      for (int k = 0; k < nBoxes[j]; ++k) {
+        Box& B = T[j][k];
+        conv(B.L2P, j < depth ? isig + loff[j + 1][4 * k] : nullptr, sig + loff[j][k]);
+        conv(B.P2M, tau + moff[j][k], j < depth ? itau + moff[j + 1][4 * k] : nullptr);
+        for (auto& kv : B.M2L) conv(kv.second, isig + loff[j][k], itau + moff[j][kv.first]);
+        for (auto& kv : B.P2P) {
+          if (j != depth && kv.second.size()) throw Fail(AIFMM_ERR_STATE, "non-leaf P2P before the elimination");
+          conv(kv.second, nullptr, nullptr);
+        }
+        for (auto* m : {&B.M2P, &B.P2L, &B.P2M_f, &B.M2M_f})
+          for (auto& kv : *m)
+            if (kv.second.size()) throw Fail(AIFMM_ERR_STATE, "elimination blocks before the elimination");
+        if ((int)ged.size() > 20000) flush_geam();
+      }
+    flush_geam();
+  }
   void snapshot_restore() {
     if (!have_saved) {
       saved.assign(depth + 1, {});
@@ -2814,11 +2993,15 @@ struct aifmm_problem {
           Box& B = T[j][k];
           Saved& S = saved[j][k];
           S.NumM = B.NumM; S.NumL = B.NumL;
-          S.L2P = newblk(B.L2P.r, B.L2P.c); copy(S.L2P, B.L2P);
-          S.P2M = newblk(B.P2M.r, B.P2M.c); copy(S.P2M, B.P2M);
-          for (auto& kv : B.M2L) { Blk t = newblk(kv.second.r, kv.second.c); copy(t, kv.second); S.M2L[kv.first] = t; }
+          S.L2P = newblk(B.L2P.r, B.L2P.c, 16); copy(S.L2P, B.L2P);
+          S.P2M = newblk(B.P2M.r, B.P2M.c, 16); copy(S.P2M, B.P2M);
+          for (auto& kv : B.M2L) { Blk t = newblk(kv.second.r, kv.second.c, 16); copy(t, kv.second); S.M2L[kv.first] = t; }
           if (j == depth)
-            for (auto& kv : B.P2P) { Blk t = newblk(kv.second.r, kv.second.c); copy(t, kv.second); S.P2P[kv.first] = t; }
+            for (auto& kv : B.P2P) {
+              Blk t = newblk(kv.second.r, kv.second.c, 16);
+              copy(t, kv.second);
+              S.P2P[kv.first] = t;
+            }
           if ((int)ged.size() > 20000) flush_geam();
         }
       }
@@ -3104,11 +3287,11 @@ aifmm_status aifmm_factorize_solve(aifmm_problem* p, int nrhs, const double* b, 
 
 aifmm_status aifmm_factorize(aifmm_problem* p, int precision, int flags) {
   if (!p) return AIFMM_ERR_ARG;
-  if (precision != AIFMM_PRECISION_FP64) {
-    p->err = "only AIFMM_PRECISION_FP64 factorisations are available";
+  if (precision != AIFMM_PRECISION_FP64 && precision != AIFMM_PRECISION_C64) {
+    p->err = "precision must be AIFMM_PRECISION_FP64 or AIFMM_PRECISION_C64";
     return AIFMM_ERR_ARG;
   }
-  return guard(p, [&] { p->factorize(flags); });
+  return guard(p, [&] { p->factorize(flags, precision); });
 }
 
 aifmm_status aifmm_solve(aifmm_problem* p, int nrhs, const double* b, long ldb, double* x, long ldx, void* stream,
@@ -3221,8 +3404,12 @@ aifmm_status aifmm_trim(aifmm_problem* p) {
     CK(cudaStreamSynchronize(p->st2));
     p->gb_idx.release(); p->gb_lst.release(); p->gb_segs.release();
     p->gb_ws.release(); p->gb_res.release(); p->gb_lu.release();
-    if (p->have_saved) p->release_saved();
-    p->have_saved = false;
+    // the complex128 assembly of a complex64 factorisation is what its refined
+    // solves multiply with: it stays
+    if (p->have_saved && !(p->factored && p->factor_es == 8)) {
+      p->release_saved();
+      p->have_saved = false;
+    }
     p->pool.commit_frees();
   });
 }

@@ -262,6 +262,9 @@ def main():
     ap.add_argument("--batched", type=int, default=1, help="1: also run the 64-problem batched configuration")
     ap.add_argument("--refined", type=int, default=1, help="1: also time the refined form (GMRES) on the same problem")
     ap.add_argument("--trace", type=float, default=30.0, help="seconds of the serving trace (0: skip)")
+    ap.add_argument("--mixed-serving", type=int, default=0,
+                    help="1: also run the batched configuration and the trace in the mixed form (complex64 "
+                         "factors, refined solves, FP64 refactoring where the refinement stagnates)")
     ap.add_argument("--no-kernel-profile", action="store_true",
                     help="skip the extra event-instrumented step that feeds the roofline (profiling runs)")
     args = ap.parse_args()
@@ -393,15 +396,21 @@ def main():
         except Exception as e:
             extra["refined_c3_physics"] = {"error": repr(e)}
     if args.batched and rank == 0:
-        try:
-            extra["batched_uneven"] = batched_uneven(device)
-        except Exception as e:
-            extra["batched_uneven"] = {"error": repr(e)}
+        forms = [("batched_uneven", 0)] + ([("batched_uneven_mixed", 1)] if args.mixed_serving else [])
+        for key, prec in forms:
+            try:
+                extra[key] = batched_uneven(device, precision=prec)
+            except Exception as e:
+                extra[key] = {"error": repr(e)}
+        if "unknowns_per_s" in extra.get("batched_uneven_mixed", {}):
+            extra["mixed_batched_over_plain_fp64"] = extra["batched_uneven_mixed"]["unknowns_per_s"] / value
     if args.trace > 0 and rank == 0:
-        try:
-            extra["serving_trace"] = serving_trace(device, seconds=args.trace)
-        except Exception as e:
-            extra["serving_trace"] = {"error": repr(e)}
+        forms = [("serving_trace", 0)] + ([("serving_trace_mixed", 1)] if args.mixed_serving else [])
+        for key, prec in forms:
+            try:
+                extra[key] = serving_trace(device, seconds=args.trace, precision=prec)
+            except Exception as e:
+                extra[key] = {"error": repr(e)}
     if rank == 0:
         peaks = measured_peaks()
         line = {
@@ -486,50 +495,71 @@ def solve_latency(T, K, lib, stream, device, args, nrhs_list=(1, 8, 64)):
     return out
 
 
-def _refined_run(T, K, b, factor_tol_pow, rtol):
+def _refined_run(T, K, b, factor_tol_pow, rtol, precision=0):
     """createTree + assemble + factorise (recompression tolerance 10^-factor_tol_pow,
-    assembly kept) + GMRES to rtol; host wall clock per phase."""
+    assembly kept; precision 1: complex64 factors) + GMRES to rtol; host wall clock
+    per phase."""
     T.set_factor_tolerance(factor_tol_pow)
     try:
         t0 = time.perf_counter()
         T.createTree()
         T.assemble()
         t1 = time.perf_counter()
-        T.factorize(keep_assembly=True)
+        T.factorize(keep_assembly=True, precision=precision)
         t2 = time.perf_counter()
-        x, iters, relres = T.solve_refined(b, rtol=rtol, maxit=90)
+        try:
+            x, iters, relres = T.solve_refined(b, rtol=rtol, maxit=90)
+            err = None
+        except Exception as e:  # stagnation is reported by the library, not hidden
+            x, iters, relres, err = None, None, None, str(e)
         t3 = time.perf_counter()
     finally:
         T.set_factor_tolerance(0)
-    return x, {"assemble_s": t1 - t0, "factorize_s": t2 - t1, "gmres_s": t3 - t2, "total_s": t3 - t0,
-               "gmres_iterations": iters, "relative_residual": relres}
+    out = {"assemble_s": t1 - t0, "factorize_s": t2 - t1, "gmres_s": t3 - t2, "total_s": t3 - t0,
+           "gmres_iterations": iters, "relative_residual": relres, "converged": err is None,
+           "factors": "complex64" if precision == 1 else "complex128"}
+    if err is not None:
+        out["error"] = err
+    return x, out
 
 
 def refined_vs_plain(T, K, th, plain_value, x_plain):
-    """The refined form on the benchmark problem itself: the same assembly (ACA
-    tolerance 1e-10), the factorisation at recompression tolerance 1e-6, FP64 GMRES
-    against the compressed operator to relative residual 1e-10, for the same 8
-    right-hand sides; against the plain FP64 direct solve of the timed steps."""
+    """The refined forms on the benchmark problem itself: the same assembly (ACA
+    tolerance 1e-10), the factorisation at recompression tolerance 1e-6 in complex128
+    and in complex64 (the mixed form), FP64 GMRES against the compressed operator to
+    relative residual 1e-10, for the same 8 right-hand sides; against the plain FP64
+    direct solve of the timed steps.  The mixed form's error is stated against the
+    complex128-factored refined solution of the same compressed system."""
     b = K.rhs_plane_wave(th)
-    x, out = _refined_run(T, K, b, 6, 1e-10)
     N = K.N
-    out["unknowns_per_s"] = N / out["total_s"]
-    out["plain_fp64_unknowns_per_s"] = plain_value
-    out["refined_over_plain"] = out["unknowns_per_s"] / plain_value
-    out["rel_diff_to_plain_solution"] = float(np.linalg.norm(x - x_plain) / np.linalg.norm(x_plain))
-    out["timing"] = "host wall clock of one run (tree, assembly, factorisation, GMRES with host buffers)"
-    return out
+    res = {}
+    for name, prec in (("fp64_factors", 0), ("mixed_c64_factors", 1)):
+        x, out = _refined_run(T, K, b, 6, 1e-10, precision=prec)
+        if x is not None:
+            out["unknowns_per_s"] = N / out["total_s"]
+            out["over_plain_fp64"] = out["unknowns_per_s"] / plain_value
+            out["rel_diff_to_plain_solution"] = float(np.linalg.norm(x - x_plain) / np.linalg.norm(x_plain))
+        res[name] = (x, out)
+    x64 = res["fp64_factors"][0]
+    xm, om = res["mixed_c64_factors"]
+    if xm is not None and x64 is not None:
+        om["rel_err_vs_fp64_refined"] = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
+    return {"plain_fp64_unknowns_per_s": plain_value,
+            "fp64_factors": res["fp64_factors"][1], "mixed_c64_factors": om,
+            "mixed_over_plain": om.get("over_plain_fp64"),
+            "timing": "host wall clock of one run each (tree, assembly, factorisation, GMRES with host buffers)"}
 
 
 def refined_c3(device, depth=6, nrhs=32, seed=SEED + 2):
     """The mixed-precision configuration's physics (8x8 nodes, kappa 80, disk q = 2 for
-    |x| < 0.5, NCA tolerance 1e-6, 32 plane waves, refinement to 1e-10) at depth 6
-    (262,144 unknowns), in this build's refined form: FP64 factorisation at the
-    problem's tolerance as the preconditioner of FP64 GMRES against the compressed
-    operator."""
+    |x| < 0.5, NCA tolerance 1e-6, 32 plane waves, refinement to 1e-10): factorisation
+    at the problem's tolerance in complex64 (the mixed form) and in complex128, each
+    the preconditioner of FP64 GMRES against the compressed operator.  The mixed
+    form's error is stated against the complex128-factored refined solution."""
     import aifmm_ls_b200 as A
     K = A.LSKernel(n_cheb=8, kappa=80.0, degree=6, depth=depth, tol_pow=6, q_kind="disk", q_amp=2.0, q_radius=0.5,
                    device=device)
+    res = {}
     try:
         t0 = time.perf_counter()
         K.tables_compute(round6=True)
@@ -537,15 +567,26 @@ def refined_c3(device, depth=6, nrhs=32, seed=SEED + 2):
         T = A.FMM2DTree(K)
         rng = np.random.default_rng(seed)
         b = K.rhs_plane_wave(rng.uniform(0, 2 * np.pi, nrhs))
-        x, out = _refined_run(T, K, b, 0, 1e-10)
-        xd = T.solve_factored(b)  # the direct solve alone, same factors
-        r_direct = float(np.max(np.linalg.norm(b - T.compressed_matvec(xd), axis=1) / np.linalg.norm(b, axis=1)))
+        for name, prec in (("mixed_c64_factors", 1), ("fp64_factors", 0)):
+            x, out = _refined_run(T, K, b, 0, 1e-10, precision=prec)
+            xd = T.solve_factored(b)  # the direct solve alone, same factors
+            out["direct_solve_relative_residual"] = float(
+                np.max(np.linalg.norm(b - T.compressed_matvec(xd), axis=1) / np.linalg.norm(b, axis=1)))
+            if x is not None:
+                out["unknowns_per_s"] = K.N / out["total_s"]
+            res[name] = (x, out)
+            lib = A.load()
+            lib.aifmm_trim(K.h)
     finally:
         K.close()
-    out.update({"depth": depth, "unknowns": K.N, "nrhs": nrhs, "tables_s": t_tab,
-                "unknowns_per_s": K.N / out["total_s"], "direct_solve_relative_residual": r_direct,
-                "note": "depth 6 instead of 7 (8x8 nodes); factorisation FP64 (no complex64 arithmetic is built)"})
-    return out
+    xm, om = res["mixed_c64_factors"]
+    x64, o64 = res["fp64_factors"]
+    if xm is not None and x64 is not None:
+        om["rel_err_vs_fp64_refined"] = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
+    ratio = om["unknowns_per_s"] / o64["unknowns_per_s"] if "unknowns_per_s" in om and "unknowns_per_s" in o64 else None
+    return {"depth": depth, "unknowns": K.N, "nrhs": nrhs, "tables_s": t_tab,
+            "mixed_c64_factors": om, "fp64_factors": o64, "mixed_over_fp64_factors": ratio,
+            "note": "depth 6 instead of 7 (8x8 nodes)"}
 
 
 def _random_problem(rng, depth):
@@ -560,15 +601,18 @@ def _random_problem(rng, depth):
     return dict(n_cheb=6, kappa=kappa, degree=6, depth=int(depth), tol_pow=8, **q)
 
 
-def batched_uneven(device, nprob=64, workers=4, seed=SEED + 3):
+def batched_uneven(device, nprob=64, workers=4, seed=SEED + 3, precision=0, rtol=1e-8):
     """64 independent problems of depth U{4..7}, each factored and solved for one random
     complex Gaussian right-hand side, run through the serving engine (workers drive their
     own handles and streams, so the problems overlap on the GPU; admission by device
-    memory).  Whole-job unknowns/s = total unknowns / wall time of the batch."""
+    memory).  precision 1: the mixed form (complex64 factors, each solve refined by FP64
+    GMRES to rtol); 0: FP64 factors and direct solves.  Whole-job unknowns/s = total
+    unknowns / wall time of the batch."""
     import aifmm_ls_b200 as A
     rng = np.random.default_rng(seed)
     probs = [_random_problem(rng, rng.integers(4, 8)) for _ in range(nprob)]
-    S = A.Server(device=device, workers=workers, max_batch_rhs=64, factor_workers=workers)
+    S = A.Server(device=device, workers=workers, max_batch_rhs=64, factor_workers=workers, precision=precision,
+                 rtol=rtol)
     try:
         t0 = time.perf_counter()
         fids = [S.factorize(i, **kw) for i, kw in enumerate(probs)]
@@ -578,9 +622,12 @@ def batched_uneven(device, nprob=64, workers=4, seed=SEED + 3):
             b = rng.standard_normal((1, N)) + 1j * rng.standard_normal((1, N))
             sids.append(S.solve(i, b))
         bad = 0
+        codes = {}
         for r in fids + sids:
             st = S.wait(r, timeout=3600)[0]
             bad += st != 0
+            if st != 0:
+                codes[str(st)] = codes.get(str(st), 0) + 1
         wall = time.perf_counter() - t0
         stats = S.stats()
     finally:
@@ -588,7 +635,9 @@ def batched_uneven(device, nprob=64, workers=4, seed=SEED + 3):
     unknowns = sum(4 ** kw["depth"] * 36 for kw in probs)
     depths = [kw["depth"] for kw in probs]
     return {"problems": nprob, "depth_counts": {str(d): depths.count(d) for d in range(4, 8)},
+            "form": "mixed: complex64 factors, refined to %g" % rtol if precision == 1 else "plain FP64",
             "unknowns": unknowns, "wall_s": wall, "unknowns_per_s": unknowns / wall, "failed": bad,
+            "failed_status_counts": codes,
             "workers": workers, "timing": "host wall clock around the whole batch (several streams)",
             "server": stats}
 
@@ -629,16 +678,18 @@ class _PlaneWaves:
         return -kw["kappa"] ** 2 * q[None, :] * np.exp(1j * ph)
 
 
-def serving_trace(device, seconds=30.0, rate=200.0, workers=8, seed=SEED + 4):
+def serving_trace(device, seconds=30.0, rate=200.0, workers=8, seed=SEED + 4, precision=0, rtol=1e-8):
     """Poisson arrivals at `rate` req/s for `seconds`: 5% factorize requests for new
     geometries (depth 5, problem as the batched configuration), 95% solve requests
     of U{1..64} plane waves against a random geometry already submitted.  Latency =
     submission to completion (host clock); the engine batches the solves queued for
-    a geometry."""
+    a geometry.  precision 1: the mixed form (complex64 factors, each solve refined to
+    rtol); 0: FP64 factors and direct solves."""
     import aifmm_ls_b200 as A
     rng = np.random.default_rng(seed)
     waves = _PlaneWaves(A)
-    S = A.Server(device=device, workers=workers, max_batch_rhs=64, factor_workers=workers // 2)
+    S = A.Server(device=device, workers=workers, max_batch_rhs=64, factor_workers=workers // 2, precision=precision,
+                 rtol=rtol)
     lat = {"solve": [], "factorize": []}
     try:
         keys = []
@@ -672,6 +723,7 @@ def serving_trace(device, seconds=30.0, rate=200.0, workers=8, seed=SEED + 4):
                 b = waves(kw, rng.uniform(0, 2 * np.pi, nr))
                 pending.append(("solve", S.solve(key, b), b.size))
         failed = 0
+        codes = {}
         for kind, rid, nunk in pending:
             st, ms, br, _ = S.wait(rid, timeout=3600)
             if st == 0:
@@ -679,11 +731,14 @@ def serving_trace(device, seconds=30.0, rate=200.0, workers=8, seed=SEED + 4):
                 solved_unknowns += nunk
             else:
                 failed += 1
+                codes[str(st)] = codes.get(str(st), 0) + 1
         wall = time.perf_counter() - t0
         stats = S.stats()
     finally:
         S.close()
     out = {"seconds": seconds, "rate_req_per_s": rate, "requests": nreq, "failed": failed, "wall_s": wall,
+           "failed_status_counts": codes,
+           "form": "mixed: complex64 factors, refined to %g" % rtol if precision == 1 else "plain FP64",
            "rhs_unknowns_per_s": solved_unknowns / wall, "server": stats,
            "note": "trace shortened from 10 minutes to keep the benchmark within minutes; new geometries at "
                    "depth 5 (a depth-7 factorisation takes seconds, longer than the mean gap between factorize "

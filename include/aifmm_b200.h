@@ -45,8 +45,12 @@ enum { AIFMM_PTR_HOST = 0, AIFMM_PTR_DEVICE = 1,
  * device until the factors are dropped (build_tree / assemble / factorize / destroy). */
 enum { AIFMM_SOLVE_GRAPH = 4 };
 
-/* Factorisation precision (aifmm_factorize). */
-enum { AIFMM_PRECISION_FP64 = 0 };
+/* Factorisation precision (aifmm_factorize).  FP64: complex128 throughout, the
+ * reference's arithmetic.  C64: the mixed form -- the elimination, its factors and
+ * aifmm_solve run in complex64 (recompression tolerance at least 1e-6); the assembly,
+ * the compressed product and aifmm_solve_refined's GMRES stay complex128, so a
+ * refined solve recovers FP64 accuracy against the compressed matrix. */
+enum { AIFMM_PRECISION_FP64 = 0, AIFMM_PRECISION_C64 = 1 };
 
 /* Contrast functions q(x): 0..5 are the reference's Qchoice values
  * (LS/LS_functions.hpp:99-112: gaussian 1.5 exp(-160|x|^2), multipleGaussians,
@@ -136,7 +140,7 @@ aifmm_status aifmm_factorize_solve(aifmm_problem* p, int nrhs, const double* b, 
  * right-hand side: the factors (QR of every P2P[k][k] and L2M_f, the fill-in
  * blocks the right-hand side passes through, the base-level QR) stay on the
  * device until the next build_tree / assemble / factorize.  precision:
- * AIFMM_PRECISION_FP64.  flags: AIFMM_KEEP_ASSEMBLY. */
+ * AIFMM_PRECISION_FP64 or AIFMM_PRECISION_C64.  flags: AIFMM_KEEP_ASSEMBLY. */
 aifmm_status aifmm_factorize(aifmm_problem* p, int precision, int flags);
 /* The right-hand-side half of the reference's solve with kept factors:
  * assign_Leaf_rhs, the right-hand-side updates of eliminate_x / eliminate_z
@@ -169,10 +173,12 @@ aifmm_status aifmm_set_factor_tolerance(aifmm_problem* p, int tol_pow);
  * column strides ldx, ldy; host or device memory (flags). */
 aifmm_status aifmm_compressed_matvec(aifmm_problem* p, int nrhs, const double* x, long ldx, double* y, long ldy,
                                      int flags);
-/* No counterpart in the reference: right-preconditioned restarted GMRES (restart 30) on
- * A_c x = b in FP64, with the kept factorisation as the preconditioner and the direct
- * solve as the starting guess, until every column's relative residual
- * ||b - A_c x|| / ||b|| <= rtol or maxit preconditioned products.  Needs
+/* No counterpart in the reference: right-preconditioned restarted GMRES (restart 30; with
+ * complex64 factors the first cycle is 10) on A_c x = b in FP64, with the kept factorisation as the preconditioner
+ * and the direct solve as the starting guess, until every column's relative residual
+ * ||b - A_c x|| / ||b|| <= rtol or maxit preconditioned products.  A restart cycle that
+ * does not halve the worst true residual ends the solve with AIFMM_ERR_NUMERIC (the
+ * factors are not an effective preconditioner; x is not written).  Needs
  * aifmm_factorize(p, precision, AIFMM_KEEP_ASSEMBLY).  *iterations and *relres (the
  * worst column's final relative residual) may be NULL.  b, x as aifmm_solve. */
 aifmm_status aifmm_solve_refined(aifmm_problem* p, int nrhs, const double* b, long ldb, double* x, long ldx,
@@ -185,7 +191,8 @@ aifmm_status aifmm_find_error(aifmm_problem* p, int nrhs, const double* x, long 
 
 /* No counterpart in the reference: return the assembly's reusable workspaces and the
  * kept copy of the assembled blocks (AIFMM_KEEP_ASSEMBLY) to the device, keeping the
- * factors.  For a handle that from now on only solves (a cached factorisation). */
+ * factors.  For a handle that from now on only solves (a cached factorisation).  After
+ * a complex64 factorisation the kept copy stays: its refined solves need it. */
 aifmm_status aifmm_trim(aifmm_problem* p);
 
 /* No counterpart in the reference (its products are Eigen expressions inside the
@@ -261,6 +268,12 @@ aifmm_status aifmm_server_destroy(aifmm_server* s);
 /* How many workers may run factorisations at once (default: all but one, so that
  * solves are never all stuck behind factorisations; 1 worker: that one). */
 aifmm_status aifmm_server_set_factor_workers(aifmm_server* s, int n);
+/* The form of the factorisations admitted from now on: AIFMM_PRECISION_FP64 (direct
+ * solves with FP64 factors, the default) or AIFMM_PRECISION_C64 (complex64 factors
+ * kept with the complex128 assembly; every solve is aifmm_solve_refined to relative
+ * residual rtol; a key whose refinement stagnates is refactored in FP64 from its kept
+ * assembly and refined again).  Keys factored earlier keep their form. */
+aifmm_status aifmm_server_set_form(aifmm_server* s, int precision, double rtol);
 /* Queue a factorisation of desc under key (tables with the 6-digit round trip, tree,
  * assembly, FP64 factorisation); replaces an earlier one under the same key. */
 aifmm_status aifmm_server_factorize(aifmm_server* s, long long key, const aifmm_desc* desc, long* request);
@@ -278,7 +291,8 @@ aifmm_status aifmm_server_wait(aifmm_server* s, long request, double timeout_s, 
 /* [0] p50 and [1] p99 solve latency (ms), [2] p50 and [3] p99 factorisation latency,
  * [4] solves and [5] factorisations completed, [6] evictions, [7] solve batches,
  * [8] mean right-hand sides per batch, [9] device bytes held by factors, [10] resident
- * factorisations, [11] failed requests.  n <= 12 values are written. */
+ * factorisations, [11] failed requests, [12] mean GMRES iterations per refined batch,
+ * [13] mixed-form keys refactored in FP64.  n <= 14 values are written. */
 aifmm_status aifmm_server_stats(aifmm_server* s, double* out, int n);
 
 #ifdef __cplusplus

@@ -121,3 +121,53 @@ def test_failed_requests_do_not_stop_the_server():
         assert S.stats()["failed"] == 2
     finally:
         S.close()
+
+
+def test_mixed_form_results_alone_and_in_the_mix():
+    """The mixed form (complex64 factors, each solve refined to relative residual
+    1e-8 against the compressed product): every result in the mix meets that
+    residual on a handle of its own and agrees with the same right-hand side
+    solved alone to the tolerance times the conditioning.  The depth-4 key's
+    complex64 refinement stagnates, so the server refactors it in FP64."""
+    import aifmm_ls_b200 as A
+    rtol = 1e-8
+    S = A.Server(workers=3, max_batch_rhs=16, precision=A.PRECISION_C64, rtol=rtol)
+    try:
+        for key, kw in PROBLEMS.items():
+            S.factorize(key, **kw)
+        rng = np.random.default_rng(21)
+        jobs = [(int(rng.integers(1, 4)), int(rng.integers(1, 4)), s) for s in range(12)]
+        rhs = {s: _rhs(key, nr, 300 + s) for key, nr, s in jobs}
+        ids = {s: (key, S.solve(key, rhs[s])) for key, nr, s in jobs}
+        out = {}
+        for s, (key, rid) in ids.items():
+            st, lat, br, x = S.wait(rid)
+            assert st == 0, st
+            out[s] = x
+        stats = S.stats()
+        print("server (mixed):", stats)
+        assert stats["solves"] == len(jobs) and stats["mean_gmres_iterations"] >= 1
+        assert stats["promoted_to_fp64"] >= 1
+    finally:
+        S.close()
+    handles = {}
+    for key, nr, s in jobs:
+        if key not in handles:
+            K = A.LSKernel(**PROBLEMS[key])
+            K.tables_compute(round6=True)
+            T = A.FMM2DTree(K)
+            T.createTree()
+            T.assemble()
+            T.factorize(keep_assembly=True, precision=A.PRECISION_C64)
+            handles[key] = (K, T)
+        K, T = handles[key]
+        b = rhs[s]
+        try:
+            x_alone, iters, relres = T.solve_refined(b, rtol=rtol, maxit=90)
+        except A.AifmmError:  # as the server does: FP64 factors from the kept assembly
+            T.factorize(keep_assembly=True, precision=A.PRECISION_FP64)
+            x_alone, iters, relres = T.solve_refined(b, rtol=rtol, maxit=90)
+        res = np.max(np.linalg.norm(b - T.compressed_matvec(out[s]), axis=1) / np.linalg.norm(b, axis=1))
+        diff = np.linalg.norm(out[s] - x_alone) / np.linalg.norm(x_alone)
+        assert res <= 1.5 * rtol, (key, s, res)
+        assert diff <= 1e-6, (key, s, diff)
