@@ -72,6 +72,7 @@ SIGNATURES = {
     "aifmm_zgemm": ([_v, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, _d, ctypes.c_int,
                      _d, ctypes.c_int, _d, _d, ctypes.c_int, ctypes.c_int], ctypes.c_int),
     "aifmm_trim": ([_v], ctypes.c_int),
+    "aifmm_release_workspaces": ([_v], ctypes.c_int),
     "aifmm_set_factor_tolerance": ([_v, ctypes.c_int], ctypes.c_int),
     "aifmm_autotune": ([_v, _d, _i], ctypes.c_int),
     "aifmm_compressed_matvec": ([_v, ctypes.c_int, _d, ctypes.c_long, _d, ctypes.c_long, ctypes.c_int], ctypes.c_int),

@@ -25,8 +25,10 @@
 //     solve refined by GMRES against the compressed product to a relative
 //     residual.  A column's refined result does not depend on its batch beyond
 //     that tolerance (the columns iterate in lockstep until the worst converges).
-//     When the refinement stagnates (complex64 factors of a deep tree), the key
-//     is refactored in FP64 from its kept assembly and the batch refined again.
+//     Complex64 factors serve trees up to depth 3, FP64 factors deeper ones
+//     (measured: complex64 factors of a deeper tree do not precondition); when a
+//     refinement stagnates all the same, the key is refactored in FP64 from its
+//     kept assembly and the batch refined again.
 // Failures (bad descriptions, a factorisation that cannot fit, CUDA errors) end
 // the request with a status; the server keeps running.
 #include <algorithm>
@@ -121,14 +123,18 @@ struct aifmm_server {
   // ~20 GB of ACA workspace during its assembly, ~65 KB per unknown in all,
   // scaled by the points per leaf.  Once factored, the measured footprint (the
   // workspace returned) replaces the estimate.
-  // The mixed form holds the complex128 assembly next to the live blocks while it
-  // converts them to complex64: about 1.7 times that peak.
-  static size_t estimate(const aifmm_desc& d, int precision) {
+  // The refined (mixed) form keeps the complex128 assembly next to the factors
+  // and holds a second copy of the blocks while it factorises: about 1.7 times
+  // the plain peak.
+  static size_t estimate(const aifmm_desc& d, bool refine) {
     const double rank = (double)d.n_cheb * d.n_cheb;
     const double N = std::ldexp(1.0, 2 * d.depth) * rank;
-    const double per = precision == AIFMM_PRECISION_C64 ? 3000.0 : 1800.0;
+    const double per = refine ? 3000.0 : 1800.0;
     return (size_t)(N * rank * per) + (size_t(64) << 20);
   }
+  // complex64 factors precondition trees up to this depth (measured: at depth 4
+  // the elimination's internal growth times FP32 rounding stalls the refinement)
+  static constexpr int kC64MaxDepth = 3;
   size_t in_use() const {
     size_t s = 0;
     for (auto& kv : factors) s += kv.second.ready ? kv.second.bytes : kv.second.reserve;
@@ -179,9 +185,9 @@ struct aifmm_server {
     if ((st = aifmm_build_tree(p)) != AIFMM_OK) return fail(st);
     if ((st = aifmm_assemble(p)) != AIFMM_OK) return fail(st);
     if ((st = aifmm_autotune(p, nullptr, nullptr)) != AIFMM_OK) return fail(st);  // tile widths for this problem
-    const int flags = f.precision == AIFMM_PRECISION_C64 ? AIFMM_KEEP_ASSEMBLY : 0;
-    if ((st = aifmm_factorize(p, f.precision, flags)) != AIFMM_OK) return fail(st);
-    if ((st = aifmm_trim(p)) != AIFMM_OK) return fail(st);
+    if ((st = aifmm_factorize(p, f.precision, f.refine ? AIFMM_KEEP_ASSEMBLY : 0)) != AIFMM_OK) return fail(st);
+    // a refined key keeps the complex128 assembly its refinement multiplies with
+    if ((st = f.refine ? aifmm_release_workspaces(p) : aifmm_trim(p)) != AIFMM_OK) return fail(st);
     double v[15] = {0};
     aifmm_stats(p, v, 15);
     bytes = (size_t)(v[13] + v[14]);
@@ -208,7 +214,7 @@ struct aifmm_server {
         Req* r = *it;
         Factor& f = factors[r->key];
         if (f.busy) { ++it; continue; }
-        const size_t need = estimate(r->desc, precision);
+        const size_t need = estimate(r->desc, precision == AIFMM_PRECISION_C64);
         if (need > budget) {  // can never fit
           it = factor_q.erase(it);
           f.queued_factor = false;
@@ -249,10 +255,10 @@ struct aifmm_server {
       if (fr) {
         Factor& f = factors[fr->key];
         f.desc = fr->desc;
-        f.precision = precision;
         f.refine = precision == AIFMM_PRECISION_C64;
+        f.precision = f.refine && f.desc.depth <= kC64MaxDepth ? AIFMM_PRECISION_C64 : AIFMM_PRECISION_FP64;
         f.rtol = rtol;
-        const size_t need = estimate(f.desc, f.precision);
+        const size_t need = estimate(f.desc, f.refine);
         f.busy = true;
         f.reserve = need;
         ++factoring;
@@ -317,8 +323,9 @@ struct aifmm_server {
       std::string err;
       const bool refine = f.refine;
       bool promoted = false;
+      double relres = 0;
       aifmm_status st =
-          refine ? aifmm_solve_refined(p, width, B.data(), N, X.data(), N, f.rtol, 90, &iters, nullptr, AIFMM_PTR_HOST)
+          refine ? aifmm_solve_refined(p, width, B.data(), N, X.data(), N, f.rtol, 90, &iters, &relres, AIFMM_PTR_HOST)
                  : aifmm_solve(p, width, B.data(), N, X.data(), N, nullptr, AIFMM_PTR_HOST | AIFMM_SOLVE_GRAPH);
       if (refine && st == AIFMM_ERR_NUMERIC && f.precision == AIFMM_PRECISION_C64) {
         // complex64 factors that do not precondition this problem (a deep tree's
@@ -328,7 +335,7 @@ struct aifmm_server {
         bool room;
         {
           std::lock_guard<std::mutex> g(mu);
-          room = make_room(estimate(f.desc, AIFMM_PRECISION_FP64), skey);
+          room = make_room(estimate(f.desc, true), skey);
         }
         if (!room) {
           st = AIFMM_ERR_NOMEM;
@@ -336,9 +343,14 @@ struct aifmm_server {
         } else {
           st = aifmm_factorize(p, AIFMM_PRECISION_FP64, AIFMM_KEEP_ASSEMBLY);
           if (st == AIFMM_OK)
-            st = aifmm_solve_refined(p, width, B.data(), N, X.data(), N, f.rtol, 90, &iters, nullptr, AIFMM_PTR_HOST);
+            st = aifmm_solve_refined(p, width, B.data(), N, X.data(), N, f.rtol, 90, &iters, &relres, AIFMM_PTR_HOST);
           promoted = true;
         }
+      }
+      if (refine && st == AIFMM_OK && !(relres <= f.rtol)) {  // the form promises rtol: say when it is not met
+        st = AIFMM_ERR_NUMERIC;
+        err = "refinement reached relative residual " + std::to_string(relres) + " in " + std::to_string(iters) +
+              " iterations, above the form's target";
       }
       if (st != AIFMM_OK && err.empty()) err = aifmm_last_error(p);
       double v[15] = {0};

@@ -127,6 +127,19 @@ class Pool {
     while (s < bytes && s < (size_t(512) << 20)) s <<= 1;
     slab_ = s;
   }
+  // return the large blocks that sit in the free lists to the device (the
+  // caller has synchronised every stream that used them)
+  void release_free_big() {
+    for (auto& kv : free_) {
+      if (kv.first <= (size_t(64) << 20)) continue;
+      for (void* p : kv.second) {
+        cudaFree(p);
+        for (size_t i = 0; i < big_.size(); ++i)
+          if (big_[i].first == p) { big_.erase(big_.begin() + (long)i); break; }
+      }
+      kv.second.clear();
+    }
+  }
   size_t reserved() const {
     size_t b = slab_bytes_;
     for (auto& kv : big_) b += kv.second;
@@ -134,7 +147,15 @@ class Pool {
   }
 
  private:
-  static size_t cls(size_t b) { size_t c = 256; while (c < b) c <<= 1; return c; }
+  // powers of two up to the slab's largest block, multiples of 64 MB above (a
+  // large buffer -- a Krylov basis -- would otherwise round up to twice its size)
+  static size_t cls(size_t b) {
+    const size_t g = size_t(64) << 20;
+    if (b > g) return (b + g - 1) / g * g;
+    size_t c = 256;
+    while (c < b) c <<= 1;
+    return c;
+  }
   std::vector<void*> slabs_;
   size_t slab_ = size_t(512) << 20, slab_bytes_ = 0;
   std::vector<std::pair<void*, size_t>> big_;
@@ -2780,11 +2801,11 @@ struct aifmm_problem {
       worst = 0;
       for (int c = 0; c < nr; ++c) { beta[c] = std::sqrt(d[c].x); worst = std::max(worst, beta[c] / bn[c]); }
       if (worst <= rtol || it >= maxit) break;
-      // A cycle that does not halve the true residual means the preconditioner is
-      // not the linear operator GMRES assumes (complex64 factors of a deep tree:
+      // With complex64 factors, a cycle that does not halve the true residual means
+      // the preconditioner is not the linear operator GMRES assumes (a deep tree:
       // the elimination's internal growth times FP32 rounding): stop rather than
       // iterate to maxit.
-      if (cycle > 0 && !(worst <= 0.5 * worst_prev)) {
+      if (factor_es == 8 && cycle > 0 && !(worst <= 0.5 * worst_prev)) {
         gm_iters = it;
         gm_relres = worst;
         throw Fail(AIFMM_ERR_NUMERIC, "GMRES refinement stagnates: relative residual " + std::to_string(worst) +
@@ -3360,7 +3381,22 @@ aifmm_status aifmm_solve_refined(aifmm_problem* p, int nrhs, const double* b, lo
   if (!p || !b || !x || nrhs < 1) return AIFMM_ERR_ARG;
   return guard(p, [&] {
     p->cur = p->st;
-    p->refine_solve(nrhs, b, ldb, x, ldx, flags, rtol, maxit, 30);
+    // the Krylov basis (31 vectors of N x nrhs) goes back to the device afterwards
+    auto give_back = [&] {
+      cudaStreamSynchronize(p->st);
+      cudaStreamSynchronize(p->st2);
+      p->pool.commit_frees();
+      p->pool.release_free_big();
+    };
+    try {
+      p->refine_solve(nrhs, b, ldb, x, ldx, flags, rtol, maxit, 30);
+    } catch (...) {
+      if (iterations) *iterations = p->gm_iters;
+      if (relres) *relres = p->gm_relres;
+      give_back();
+      throw;
+    }
+    give_back();
     if (iterations) *iterations = p->gm_iters;
     if (relres) *relres = p->gm_relres;
   });
@@ -3411,6 +3447,7 @@ aifmm_status aifmm_trim(aifmm_problem* p) {
       p->have_saved = false;
     }
     p->pool.commit_frees();
+    p->pool.release_free_big();
   });
 }
 
@@ -3445,6 +3482,18 @@ aifmm_status aifmm_zgemm(aifmm_problem* p, int opA, int opB, int m, int n, int k
     p->flush_gemm();
     if (!dev) CK(cudaMemcpyAsync(C, dC, bC, cudaMemcpyDeviceToHost, p->st));
     p->sync();
+  });
+}
+
+aifmm_status aifmm_release_workspaces(aifmm_problem* p) {
+  if (!p) return AIFMM_ERR_ARG;
+  return guard(p, [&] {
+    p->sync();
+    CK(cudaStreamSynchronize(p->st2));
+    p->gb_idx.release(); p->gb_lst.release(); p->gb_segs.release();
+    p->gb_ws.release(); p->gb_res.release(); p->gb_lu.release();
+    p->pool.commit_frees();
+    p->pool.release_free_big();
   });
 }
 

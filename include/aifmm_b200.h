@@ -194,6 +194,10 @@ aifmm_status aifmm_find_error(aifmm_problem* p, int nrhs, const double* x, long 
  * factors.  For a handle that from now on only solves (a cached factorisation).  After
  * a complex64 factorisation the kept copy stays: its refined solves need it. */
 aifmm_status aifmm_trim(aifmm_problem* p);
+/* No counterpart in the reference: return the assembly's reusable workspaces only; the
+ * kept copy of the assembled blocks stays (for aifmm_solve_refined and
+ * aifmm_compressed_matvec on a handle that keeps its factors). */
+aifmm_status aifmm_release_workspaces(aifmm_problem* p);
 
 /* No counterpart in the reference (its products are Eigen expressions inside the
  * elimination, e.g. FMM2DTree_find_error.hpp:1961-2075): the solver's batched complex
@@ -270,9 +274,11 @@ aifmm_status aifmm_server_destroy(aifmm_server* s);
 aifmm_status aifmm_server_set_factor_workers(aifmm_server* s, int n);
 /* The form of the factorisations admitted from now on: AIFMM_PRECISION_FP64 (direct
  * solves with FP64 factors, the default) or AIFMM_PRECISION_C64 (complex64 factors
- * kept with the complex128 assembly; every solve is aifmm_solve_refined to relative
- * residual rtol; a key whose refinement stagnates is refactored in FP64 from its kept
- * assembly and refined again).  Keys factored earlier keep their form. */
+ * kept with the complex128 assembly for trees of depth <= 3, FP64 factors kept with it
+ * for deeper trees -- complex64 factors do not precondition those, measured -- and every
+ * solve aifmm_solve_refined to relative residual rtol; a key whose complex64 refinement
+ * stagnates is refactored in FP64 from its kept assembly and refined again).  Keys
+ * factored earlier keep their form. */
 aifmm_status aifmm_server_set_form(aifmm_server* s, int precision, double rtol);
 /* Queue a factorisation of desc under key (tables with the 6-digit round trip, tree,
  * assembly, FP64 factorisation); replaces an earlier one under the same key. */
