@@ -118,18 +118,17 @@ struct aifmm_server {
   long evictions = 0, batches = 0, batch_rhs_total = 0, rejected = 0;
 
   // Device bytes a factorisation of this description may hold at its peak: the
-  // 6x6-node depth-7 benchmark problem holds ~17 GiB of blocks (~31 KB per
-  // unknown: rank x rank blocks per neighbour and interaction-list entry) plus
-  // ~20 GB of ACA workspace during its assembly, ~65 KB per unknown in all,
-  // scaled by the points per leaf.  Once factored, the measured footprint (the
-  // workspace returned) replaces the estimate.
+  // 6x6-node depth-7 benchmark problem holds its blocks (the pool) plus the
+  // assembly's chunked ACA buffers (at most a few GB), scaled by the points per
+  // leaf.  Once factored, the measured footprint (the workspaces returned)
+  // replaces the estimate.
   // The refined (mixed) form keeps the complex128 assembly next to the factors
   // and holds a second copy of the blocks while it factorises: about 1.7 times
   // the plain peak.
   static size_t estimate(const aifmm_desc& d, bool refine) {
     const double rank = (double)d.n_cheb * d.n_cheb;
     const double N = std::ldexp(1.0, 2 * d.depth) * rank;
-    const double per = refine ? 3000.0 : 1800.0;
+    const double per = refine ? 1900.0 : 1100.0;
     return (size_t)(N * rank * per) + (size_t(64) << 20);
   }
   // complex64 factors precondition trees up to this depth (measured: at depth 4

@@ -431,7 +431,9 @@ struct aifmm_problem {
   Pool pool;
   Arena scratch;
   Staging stage;
-  GrowBuf gb_idx, gb_lst, gb_segs, gb_ws, gb_res, gb_lu;
+  GrowBuf gb_idx, gb_lst, gb_segs, gb_ws, gb_res, gb_lu, gb_acf;
+  // the ACA of a level runs in chunks of boxes whose workspace and factors fit this
+  static constexpr size_t kAcaChunkBytes = size_t(2) << 30;
   // timings / counters
   double ms[4] = {0, 0, 0, 0};
   long launches_ = 0, launches_fs = 0, launches_asm = 0;
@@ -1121,152 +1123,186 @@ struct aifmm_problem {
         CK(cudaMemcpyAsync(d_segs, segs.data(), sizeof(int4) * segs.size(), cudaMemcpyHostToDevice, st));
         KL(aifmm_launch_gather_segments(d_lst, d_segs, (long)segs.size(), d_idx, st));
       }
-      // ---- workspaces
-      size_t ws = 0, nres = 0;
-      std::vector<size_t> wo(2 * nbx), ro(2 * nbx);
-      for (int t = 0; t < 2 * nbx; ++t) {
+      // ---- the level's boxes in chunks: a chunk's ACA workspace and unmodified
+      // rows / columns (Ac, Ar: read only by the chunk's interpolative operators)
+      // live in reusable buffers of at most kAcaChunkBytes, so the assembly's peak
+      // does not grow with the number of boxes of a level.  Every job is computed
+      // as in one launch per level.
+      auto job_bytes = [&](int t, size_t& wsb, size_t& acb) {
         const int n1 = ji[t].n1, n2 = ji[t].n2, rmax = std::min(n1, n2);
         const int np = n1 < n2 ? n1 : n2, ns = n1 < n2 ? n2 : n1;
-        wo[t] = ws;
-        size_t b = sizeof(double2) * ((size_t)rmax * np + (size_t)rmax * ns + ns + np + 3 * (size_t)rmax + 3) + np + ns + 16;
-        ws += (b + 255) & ~size_t(255);
-        ro[t] = nres;
-        nres += 2 * (size_t)rmax;
-      }
-      char* d_ws = static_cast<char*>(gb_ws.get(ws, st));
-      // [2 per job: rank, branch] then the bases
-      int* d_res = static_cast<int*>(gb_res.get(sizeof(int) * (2 * (size_t)2 * nbx + nres + 1), st));
-      int* d_bases = d_res + 2 * 2 * nbx;
-      std::vector<AcaJob> jobs(2 * nbx);
-      for (int t = 0; t < 2 * nbx; ++t) {
-        const int k = t / 2;
-        const bool outgoing = (t % 2) == 0;
-        const int n1 = ji[t].n1, n2 = ji[t].n2, rmax = std::min(n1, n2);
-        const int np = n1 < n2 ? n1 : n2, ns = n1 < n2 ? n2 : n1;
-        char* base = d_ws + wo[t];
-        AcaJob& J = jobs[t];
-        J.rows = d_idx + ji[t].r0; J.cols = d_idx + ji[t].c0; J.n1 = n1; J.n2 = n2;
-        J.want_rows = outgoing ? 1 : 0;
-        J.U = reinterpret_cast<double2*>(base); base += sizeof(double2) * (size_t)rmax * np;
-        J.V = reinterpret_cast<double2*>(base); base += sizeof(double2) * (size_t)rmax * ns;
-        J.P = reinterpret_cast<double2*>(base); base += sizeof(double2) * ns;
-        J.S = reinterpret_cast<double2*>(base); base += sizeof(double2) * np;
-        J.coef = reinterpret_cast<double2*>(base); base += sizeof(double2) * (rmax + 1);
-        J.dots_u = reinterpret_cast<double2*>(base); base += sizeof(double2) * (rmax + 1);
-        J.dots_v = reinterpret_cast<double2*>(base); base += sizeof(double2) * (rmax + 1);
-        J.remP = reinterpret_cast<unsigned char*>(base); base += np;
-        J.remS = reinterpret_cast<unsigned char*>(base);
-        J.rank = d_res + 2 * t;
-        J.prim_bases = d_bases + ro[t];
-        J.sec_bases = d_bases + ro[t] + rmax;
-        Box& B = T[j][k];
-        if (outgoing) { drop(B.Ar); B.Ar = newblk(rmax, n2); J.out = B.Ar.p.d(); B.Ar.ld = std::max(rmax, 1); }
-        else { drop(B.Ac); B.Ac = newblk(n1, rmax); J.out = B.Ac.p.d(); }
-      }
+        const size_t b = sizeof(double2) * ((size_t)rmax * np + (size_t)rmax * ns + ns + np + 3 * (size_t)rmax + 3) + np + ns + 16;
+        wsb = (b + 255) & ~size_t(255);
+        acb = (sizeof(double2) * (size_t)rmax * ((t % 2) == 0 ? n2 : n1) + 255) & ~size_t(255);
+      };
       st_asm_lists_ms += since(ta);
-      ta = clk::now();
-      const AcaJob* dj = stage.put(jobs, st);
-      CK(cudaEventRecord(ea, st));
-      KL(aifmm_launch_aca(dj, (int)jobs.size(), tol, cx, st));
-      CK(cudaEventRecord(eb, st));
-      // ---- ranks and skeletons back to the host
-      std::vector<int> hres(2 * (size_t)2 * nbx + nres + 1);
-      CK(cudaMemcpyAsync(hres.data(), d_res, sizeof(int) * hres.size(), cudaMemcpyDeviceToHost, st));
-      sync();
-      std::vector<std::vector<int>> pb(2 * nbx), sb(2 * nbx);
-      std::vector<int> rk(2 * nbx), br(2 * nbx);
-      const int* hb = hres.data() + 2 * 2 * nbx;
-      for (int t = 0; t < 2 * nbx; ++t) {
-        const int rmax = std::min(ji[t].n1, ji[t].n2);
-        rk[t] = hres[2 * t]; br[t] = hres[2 * t + 1];
-        if (rk[t] < 0) throw Fail(AIFMM_ERR_NUMERIC, "ACA block too large");
-        pb[t].assign(hb + ro[t], hb + ro[t] + rk[t]);
-        sb[t].assign(hb + ro[t] + rmax, hb + ro[t] + rmax + rk[t]);
-      }
-      {
-        float ms_ = 0;
-        CK(cudaEventElapsedTime(&ms_, ea, eb));
-        st_asm_aca_gpu_ms += ms_;
-      }
-      st_asm_aca_ms += since(ta);
-      ta = clk::now();
-      // ---- skeletons, rank equalisation (F:1105-1113) and L2P / P2M jobs
-      std::vector<int> sk;  // skeleton index lists for the LU jobs
-      struct LUI { long rows, cols; };
-      std::vector<LUI> lui(2 * nbx);
-      for (int k = 0; k < nbx; ++k) {
-        Box& B = T[j][k];
-        B.in_check.clear(); B.in_charge.clear(); B.out_check.clear(); B.out_charge.clear();
-        // outgoing (t = 2k): rows = the IL boxes' in-lists, cols = k's out-list
+      for (int k0 = 0; k0 < nbx;) {
+        ta = clk::now();
+        int k1 = k0;
+        size_t ws = 0, acs = 0;
+        for (; k1 < nbx; ++k1) {
+          size_t w0, a0, w1, a1;
+          job_bytes(2 * k1, w0, a0);
+          job_bytes(2 * k1 + 1, w1, a1);
+          if (k1 > k0 && ws + w0 + w1 + acs + a0 + a1 > kAcaChunkBytes) break;
+          ws += w0 + w1;
+          acs += a0 + a1;
+        }
+        const int nch = k1 - k0, nj = 2 * nch, t0 = 2 * k0;
+        size_t nres = 0;
+        std::vector<size_t> wo(nj), ao(nj), ro(nj);
         {
-          const int t = 2 * k;
-          const auto& rb = br[t] == 1 ? pb[t] : sb[t];
-          const auto& cb = br[t] == 1 ? sb[t] : pb[t];
-          B.rank_out = rk[t];
-          for (int r : rb) B.out_check.push_back(il_point(k, true, r));
-          for (int c : cb) B.out_charge.push_back(lst[lout_off[k] + c]);
-          B.Ar.r = rk[t];
+          size_t w = 0, ac = 0;
+          for (int q = 0; q < nj; ++q) {
+            size_t wb, ab;
+            job_bytes(t0 + q, wb, ab);
+            wo[q] = w; w += wb;
+            ao[q] = ac; ac += ab;
+            ro[q] = nres;
+            nres += 2 * (size_t)std::min(ji[t0 + q].n1, ji[t0 + q].n2);
+          }
         }
-        {
-          const int t = 2 * k + 1;
-          const auto& rb = br[t] == 1 ? pb[t] : sb[t];
-          const auto& cb = br[t] == 1 ? sb[t] : pb[t];
-          B.rank_in = rk[t];
-          for (int r : rb) B.in_check.push_back(lst[lin_off[k] + r]);
-          for (int c : cb) B.in_charge.push_back(il_point(k, false, c));
-          B.Ac.c = rk[t];
+        char* d_ws = static_cast<char*>(gb_ws.get(ws, st));
+        char* d_ac = static_cast<char*>(gb_acf.get(acs, st));
+        // [2 per job: rank, branch] then the bases
+        int* d_res = static_cast<int*>(gb_res.get(sizeof(int) * (2 * (size_t)nj + nres + 1), st));
+        int* d_bases = d_res + 2 * nj;
+        std::vector<AcaJob> jobs(nj);
+        for (int q = 0; q < nj; ++q) {
+          const int t = t0 + q, k = t / 2;
+          const bool outgoing = (t % 2) == 0;
+          const int n1 = ji[t].n1, n2 = ji[t].n2, rmax = std::min(n1, n2);
+          const int np = n1 < n2 ? n1 : n2, ns = n1 < n2 ? n2 : n1;
+          char* base = d_ws + wo[q];
+          AcaJob& J = jobs[q];
+          J.rows = d_idx + ji[t].r0; J.cols = d_idx + ji[t].c0; J.n1 = n1; J.n2 = n2;
+          J.want_rows = outgoing ? 1 : 0;
+          J.U = reinterpret_cast<double2*>(base); base += sizeof(double2) * (size_t)rmax * np;
+          J.V = reinterpret_cast<double2*>(base); base += sizeof(double2) * (size_t)rmax * ns;
+          J.P = reinterpret_cast<double2*>(base); base += sizeof(double2) * ns;
+          J.S = reinterpret_cast<double2*>(base); base += sizeof(double2) * np;
+          J.coef = reinterpret_cast<double2*>(base); base += sizeof(double2) * (rmax + 1);
+          J.dots_u = reinterpret_cast<double2*>(base); base += sizeof(double2) * (rmax + 1);
+          J.dots_v = reinterpret_cast<double2*>(base); base += sizeof(double2) * (rmax + 1);
+          J.remP = reinterpret_cast<unsigned char*>(base); base += np;
+          J.remS = reinterpret_cast<unsigned char*>(base);
+          J.rank = d_res + 2 * q;
+          J.prim_bases = d_bases + ro[q];
+          J.sec_bases = d_bases + ro[q] + rmax;
+          Box& B = T[j][k];
+          double2* acp = reinterpret_cast<double2*>(d_ac + ao[q]);
+          // views into the chunk buffer (not owned: the next chunk reuses it)
+          if (outgoing) { drop(B.Ar); B.Ar = Blk{acp, rmax, n2, std::max(rmax, 1)}; J.out = acp; }
+          else { drop(B.Ac); B.Ac = Blk{acp, n1, rmax, std::max(n1, 1)}; J.out = acp; }
         }
-        const size_t r = std::min(B.in_check.size(), B.out_check.size());
-        B.in_check.resize(r); B.in_charge.resize(r); B.out_check.resize(r); B.out_charge.resize(r);
-        lui[2 * k] = {(long)sk.size(), 0};
-        sk.insert(sk.end(), B.in_check.begin(), B.in_check.end());
-        lui[2 * k].cols = (long)sk.size();
-        sk.insert(sk.end(), B.in_charge.begin(), B.in_charge.end());
-        lui[2 * k + 1] = {(long)sk.size(), 0};
-        sk.insert(sk.end(), B.out_check.begin(), B.out_check.end());
-        lui[2 * k + 1].cols = (long)sk.size();
-        sk.insert(sk.end(), B.out_charge.begin(), B.out_charge.end());
-      }
-      const int* d_sk = stage.put(sk.empty() ? std::vector<int>{0} : sk, st);
-      std::vector<SkelLUJob> lj;
-      size_t lws = 0;
-      std::vector<size_t> lwo;
-      for (int k = 0; k < nbx; ++k) {
-        Box& B = T[j][k];
-        const int r = (int)B.in_check.size();
-        const int m_in = lin_len(k), m_out = lout_len(k);
-        drop(B.L2P); drop(B.P2M);
-        B.L2P = newblk(m_in, r);
-        B.P2M = newblk(r, m_out);
-        if (r == 0) continue;
-        SkelLUJob a;  // L2P = Ac(:, :r) D1^{-1}, via LU of D1^H (F:1117-1119)
-        a.rows = d_sk + lui[2 * k].rows; a.cols = d_sk + lui[2 * k].cols; a.r = r; a.adjD = 1;
-        a.B = B.Ac.p.d(); a.ldb = B.Ac.ld; a.adjB = 1; a.m = m_in; a.X = B.L2P.p.d(); a.ldx = B.L2P.ld; a.adjX = 1;
-        lwo.push_back(lws);
-        lws += (sizeof(double2) * ((size_t)r * r + (size_t)r * m_in) + sizeof(int) * r + 511) & ~size_t(255);
-        lj.push_back(a);
-        SkelLUJob b;  // P2M = D2^{-1} Ar(:r, :) (F:1124-1126)
-        b.rows = d_sk + lui[2 * k + 1].rows; b.cols = d_sk + lui[2 * k + 1].cols; b.r = r; b.adjD = 0;
-        b.B = B.Ar.p.d(); b.ldb = B.Ar.ld; b.adjB = 0; b.m = m_out; b.X = B.P2M.p.d(); b.ldx = B.P2M.ld; b.adjX = 0;
-        lwo.push_back(lws);
-        lws += (sizeof(double2) * ((size_t)r * r + (size_t)r * m_out) + sizeof(int) * r + 511) & ~size_t(255);
-        lj.push_back(b);
-      }
-      if (!lj.empty()) {
-        char* d_lw = static_cast<char*>(gb_lu.get(lws, st));
-        for (size_t t = 0; t < lj.size(); ++t) {
-          char* base = d_lw + lwo[t];
-          const int r = lj[t].r, m = lj[t].m;
-          lj[t].work = reinterpret_cast<double2*>(base);
-          lj[t].piv = reinterpret_cast<int*>(base + sizeof(double2) * ((size_t)r * r + (size_t)r * m));
-        }
-        const SkelLUJob* dl = stage.put(lj, st);
-        KL(aifmm_launch_skel_lu(dl, (int)lj.size(), cx, st));
+        st_asm_lists_ms += since(ta);
+        ta = clk::now();
+        const AcaJob* dj = stage.put(jobs, st);
+        CK(cudaEventRecord(ea, st));
+        KL(aifmm_launch_aca(dj, nj, tol, cx, st));
+        CK(cudaEventRecord(eb, st));
+        // ---- ranks and skeletons back to the host
+        std::vector<int> hres(2 * (size_t)nj + nres + 1);
+        CK(cudaMemcpyAsync(hres.data(), d_res, sizeof(int) * hres.size(), cudaMemcpyDeviceToHost, st));
         sync();
+        std::vector<std::vector<int>> pb(nj), sb(nj);
+        std::vector<int> rk(nj), br(nj);
+        const int* hb = hres.data() + 2 * nj;
+        for (int q = 0; q < nj; ++q) {
+          const int rmax = std::min(ji[t0 + q].n1, ji[t0 + q].n2);
+          rk[q] = hres[2 * q]; br[q] = hres[2 * q + 1];
+          if (rk[q] < 0) throw Fail(AIFMM_ERR_NUMERIC, "ACA block too large");
+          pb[q].assign(hb + ro[q], hb + ro[q] + rk[q]);
+          sb[q].assign(hb + ro[q] + rmax, hb + ro[q] + rmax + rk[q]);
+        }
+        {
+          float ms_ = 0;
+          CK(cudaEventElapsedTime(&ms_, ea, eb));
+          st_asm_aca_gpu_ms += ms_;
+        }
+        st_asm_aca_ms += since(ta);
+        ta = clk::now();
+        // ---- skeletons, rank equalisation (F:1105-1113) and L2P / P2M jobs
+        std::vector<int> sk;  // skeleton index lists for the LU jobs
+        struct LUI { long rows, cols; };
+        std::vector<LUI> lui(nj);
+        for (int k = k0; k < k1; ++k) {
+          Box& B = T[j][k];
+          const int q0 = 2 * (k - k0);
+          B.in_check.clear(); B.in_charge.clear(); B.out_check.clear(); B.out_charge.clear();
+          // outgoing (job 2k): rows = the IL boxes' in-lists, cols = k's out-list
+          {
+            const int q = q0;
+            const auto& rb = br[q] == 1 ? pb[q] : sb[q];
+            const auto& cb = br[q] == 1 ? sb[q] : pb[q];
+            B.rank_out = rk[q];
+            for (int r : rb) B.out_check.push_back(il_point(k, true, r));
+            for (int c : cb) B.out_charge.push_back(lst[lout_off[k] + c]);
+            B.Ar.r = rk[q];
+          }
+          {
+            const int q = q0 + 1;
+            const auto& rb = br[q] == 1 ? pb[q] : sb[q];
+            const auto& cb = br[q] == 1 ? sb[q] : pb[q];
+            B.rank_in = rk[q];
+            for (int r : rb) B.in_check.push_back(lst[lin_off[k] + r]);
+            for (int c : cb) B.in_charge.push_back(il_point(k, false, c));
+            B.Ac.c = rk[q];
+          }
+          const size_t r = std::min(B.in_check.size(), B.out_check.size());
+          B.in_check.resize(r); B.in_charge.resize(r); B.out_check.resize(r); B.out_charge.resize(r);
+          lui[q0] = {(long)sk.size(), 0};
+          sk.insert(sk.end(), B.in_check.begin(), B.in_check.end());
+          lui[q0].cols = (long)sk.size();
+          sk.insert(sk.end(), B.in_charge.begin(), B.in_charge.end());
+          lui[q0 + 1] = {(long)sk.size(), 0};
+          sk.insert(sk.end(), B.out_check.begin(), B.out_check.end());
+          lui[q0 + 1].cols = (long)sk.size();
+          sk.insert(sk.end(), B.out_charge.begin(), B.out_charge.end());
+        }
+        const int* d_sk = stage.put(sk.empty() ? std::vector<int>{0} : sk, st);
+        std::vector<SkelLUJob> lj;
+        size_t lws = 0;
+        std::vector<size_t> lwo;
+        for (int k = k0; k < k1; ++k) {
+          Box& B = T[j][k];
+          const int q0 = 2 * (k - k0);
+          const int r = (int)B.in_check.size();
+          const int m_in = lin_len(k), m_out = lout_len(k);
+          drop(B.L2P); drop(B.P2M);
+          B.L2P = newblk(m_in, r);
+          B.P2M = newblk(r, m_out);
+          if (r == 0) continue;
+          SkelLUJob a;  // L2P = Ac(:, :r) D1^{-1}, via LU of D1^H (F:1117-1119)
+          a.rows = d_sk + lui[q0].rows; a.cols = d_sk + lui[q0].cols; a.r = r; a.adjD = 1;
+          a.B = B.Ac.p.d(); a.ldb = B.Ac.ld; a.adjB = 1; a.m = m_in; a.X = B.L2P.p.d(); a.ldx = B.L2P.ld; a.adjX = 1;
+          lwo.push_back(lws);
+          lws += (sizeof(double2) * ((size_t)r * r + (size_t)r * m_in) + sizeof(int) * r + 511) & ~size_t(255);
+          lj.push_back(a);
+          SkelLUJob b;  // P2M = D2^{-1} Ar(:r, :) (F:1124-1126)
+          b.rows = d_sk + lui[q0 + 1].rows; b.cols = d_sk + lui[q0 + 1].cols; b.r = r; b.adjD = 0;
+          b.B = B.Ar.p.d(); b.ldb = B.Ar.ld; b.adjB = 0; b.m = m_out; b.X = B.P2M.p.d(); b.ldx = B.P2M.ld; b.adjX = 0;
+          lwo.push_back(lws);
+          lws += (sizeof(double2) * ((size_t)r * r + (size_t)r * m_out) + sizeof(int) * r + 511) & ~size_t(255);
+          lj.push_back(b);
+        }
+        if (!lj.empty()) {
+          char* d_lw = static_cast<char*>(gb_lu.get(lws, st));
+          for (size_t t = 0; t < lj.size(); ++t) {
+            char* base = d_lw + lwo[t];
+            const int r = lj[t].r, m = lj[t].m;
+            lj[t].work = reinterpret_cast<double2*>(base);
+            lj[t].piv = reinterpret_cast<int*>(base + sizeof(double2) * ((size_t)r * r + (size_t)r * m));
+          }
+          const SkelLUJob* dl = stage.put(lj, st);
+          KL(aifmm_launch_skel_lu(dl, (int)lj.size(), cx, st));
+        }
+        sync();  // the chunk buffers are reused by the next chunk
+        for (int k = k0; k < k1; ++k) { Box& B = T[j][k]; B.Ac = Blk(); B.Ar = Blk(); }
+        pool.commit_frees();
+        st_asm_lu_ms += since(ta);
+        k0 = k1;
       }
-      for (int k = 0; k < nbx; ++k) { Box& B = T[j][k]; drop(B.Ac); drop(B.Ar); }
-      pool.commit_frees();
-      st_asm_lu_ms += since(ta);
     }
     auto tb = clk::now();
     // ---- M2L blocks (F:1338-1361) and leaf P2P blocks (F:1729-1741)
@@ -3439,7 +3475,7 @@ aifmm_status aifmm_trim(aifmm_problem* p) {
     p->sync();
     CK(cudaStreamSynchronize(p->st2));
     p->gb_idx.release(); p->gb_lst.release(); p->gb_segs.release();
-    p->gb_ws.release(); p->gb_res.release(); p->gb_lu.release();
+    p->gb_ws.release(); p->gb_res.release(); p->gb_lu.release(); p->gb_acf.release();
     // the complex128 assembly of a complex64 factorisation is what its refined
     // solves multiply with: it stays
     if (p->have_saved && !(p->factored && p->factor_es == 8)) {
@@ -3491,7 +3527,7 @@ aifmm_status aifmm_release_workspaces(aifmm_problem* p) {
     p->sync();
     CK(cudaStreamSynchronize(p->st2));
     p->gb_idx.release(); p->gb_lst.release(); p->gb_segs.release();
-    p->gb_ws.release(); p->gb_res.release(); p->gb_lu.release();
+    p->gb_ws.release(); p->gb_res.release(); p->gb_lu.release(); p->gb_acf.release();
     p->pool.commit_frees();
     p->pool.release_free_big();
   });
@@ -3602,6 +3638,7 @@ aifmm_status aifmm_stats(const aifmm_problem* p, double* out, int n) {
   if (!p || !out) return AIFMM_ERR_ARG;
   const double grow = (double)(p->gb_idx.capacity() + p->gb_lst.capacity() + p->gb_segs.capacity() +
                                p->gb_ws.capacity() + p->gb_res.capacity() + p->gb_lu.capacity() +
+                               p->gb_acf.capacity() +
                                p->scratch.capacity() + p->stage.cap_);
   const double v[15] = {p->st_sync_ms, (double)p->st_syncs, p->st_pending_ms, p->st_elim_ms, p->st_back_ms,
                         (double)p->st_compress, p->ms[3], (double)p->launches_fs,

@@ -80,7 +80,7 @@ def test_results_same_alone_and_in_the_mix():
 def test_lru_eviction_and_factoring_again():
     import aifmm_ls_b200 as A
     # room for one depth-3 factorisation (the server's estimate) but not two
-    est = (4 ** 3 * 36) * 36 * 1800.0 + (64 << 20)
+    est = (4 ** 3 * 36) * 36 * 1100.0 + (64 << 20)
     S = A.Server(workers=1, hbm_budget_bytes=1.5 * est)
     try:
         b1 = _rhs(1, 2, 5)
