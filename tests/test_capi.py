@@ -67,3 +67,19 @@ def test_server_refuses_to_start_without_device():
     with pytest.raises(A.AifmmError) as e:
         A.Server(workers=1)
     assert e.value.status == 6  # AIFMM_ERR_NODEVICE
+
+
+def test_entry_points_reject_null_handles():
+    """Argument checks that need no device: every handle-taking entry point of the
+    factor / solve / mixed-form / serving surface answers AIFMM_ERR_ARG (1) for a
+    NULL handle instead of touching it."""
+    import aifmm_ls_b200 as A
+    lib = A.load()
+    null = None
+    assert lib.aifmm_factorize(null, A.PRECISION_C64, 0) == 1
+    assert lib.aifmm_factorize(null, 7, 0) == 1
+    assert lib.aifmm_release_workspaces(null) == 1
+    assert lib.aifmm_trim(null) == 1
+    assert lib.aifmm_set_factor_tolerance(null, 6) == 1
+    assert lib.aifmm_server_set_form(null, A.PRECISION_C64, 1e-8) == 1
+    assert lib.aifmm_server_set_factor_workers(null, 2) == 1
