@@ -158,14 +158,27 @@ class FMM2DTree {
   // eliminate_phase_efficient (F:2407-2451) with the base-level factorisation; the
   // reference carries the right-hand side through it, here the factors are kept and
   // the right-hand side goes through back_substitution_phase
-  void eliminate_phase_efficient() {
-    check(aifmm_factorize(K_->handle(), AIFMM_PRECISION_FP64, 0), K_->handle());
+  // precision AIFMM_PRECISION_C64: the mixed form (complex64 factors; refine() recovers
+  // FP64 accuracy and needs keep_assembly)
+  void eliminate_phase_efficient(int precision = AIFMM_PRECISION_FP64, bool keep_assembly = false) {
+    check(aifmm_factorize(K_->handle(), precision, keep_assembly ? AIFMM_KEEP_ASSEMBLY : 0), K_->handle());
   }
   // the right-hand-side updates of the elimination, the base-level solve and the
   // back substitution (F:1968-2001, 2252-2293, 2453-2532) with the kept factors
   void back_substitution_phase() {
     check(aifmm_solve(K_->handle(), nrhs_, reinterpret_cast<const double*>(b_.data()), N_,
                       reinterpret_cast<double*>(x_.data()), N_, nullptr, AIFMM_PTR_HOST), K_->handle());
+  }
+  // no counterpart in the reference: GMRES refinement of the solution against the
+  // compressed operator to relative residual rtol, with the kept factors as the
+  // preconditioner (eliminate_phase_efficient(..., true) first); returns the
+  // iterations, *relres the worst column's final relative residual
+  int refine(double rtol, int maxit = 90, double* relres = nullptr) {
+    int it = 0;
+    check(aifmm_solve_refined(K_->handle(), nrhs_, reinterpret_cast<const double*>(b_.data()), N_,
+                              reinterpret_cast<double*>(x_.data()), N_, rtol, maxit, &it, relres, AIFMM_PTR_HOST),
+          K_->handle());
+    return it;
   }
   // another right-hand side against the same factors
   void set_rhs(const dtype* properties) { b_.assign(properties, properties + (size_t)N_ * nrhs_); }

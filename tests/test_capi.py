@@ -83,3 +83,29 @@ def test_entry_points_reject_null_handles():
     assert lib.aifmm_set_factor_tolerance(null, 6) == 1
     assert lib.aifmm_server_set_form(null, A.PRECISION_C64, 1e-8) == 1
     assert lib.aifmm_server_set_factor_workers(null, 2) == 1
+
+
+def test_cpp_shim_compiles_with_the_mixed_form(tmp_path):
+    """The C++ drop-in surface (include/aifmm_fmm2dtree.hpp) with the factor
+    precision and the refinement compiles against the C ABI header."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "shim.cpp"
+    src.write_text(
+        '#include "aifmm_fmm2dtree.hpp"\\n'
+        "int main() {\\n"
+        "  aifmm::FMM2DTree<aifmm::userkernel>* T = nullptr;\\n"
+        "  if (T) {\\n"
+        "    T->eliminate_phase_efficient(AIFMM_PRECISION_C64, true);\\n"
+        "    T->back_substitution_phase();\\n"
+        "    double r = 0;\\n"
+        "    T->refine(1e-10, 60, &r);\\n"
+        "  }\\n"
+        "  return 0;\\n"
+        "}\\n")
+    out = subprocess.run([cxx, "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(src)],
+                         capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
